@@ -1,0 +1,202 @@
+"""Case-file reader for the CPU oracle (test infrastructure only).
+
+An independent Python restatement of the reference's XML v3 handling and unit
+conversion, kept apart from the product's C++ reader so that the two check each
+other:
+
+* `src/configuration/SimConfig.cc:84-198` (simulation section, extra warm-up steps),
+  `:262-408` (iolets), `:640-655` (iolet position in lattice units, normalised normal),
+  `:668-723` (initial conditions, sponge layer), `:725-754` (cosine),
+  `:796-824` (WK3), `:856-876` (parabolic);
+* `src/util/UnitConverter.cc:15-118`, `src/util/UnitConverter.h:153-203`;
+* `src/lb/LbmParameters.h:29-37` (tau from dt and dx), `src/constants.h`.
+"""
+
+from __future__ import annotations
+
+import math
+import os
+import xml.etree.ElementTree as ET
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+CS2 = 1.0 / 3.0
+MMHG_TO_PASCAL = 133.3223874
+BLOOD_DENSITY = 1000.0
+BLOOD_VISCOSITY = 0.004
+REFERENCE_PRESSURE_MMHG = 0.0
+
+
+def _vec(s: str):
+    s = s.strip()
+    if not (s.startswith("(") and s.endswith(")")):
+        raise ValueError(f"bad vector {s!r}")
+    parts = [float(p) for p in s[1:-1].split(",")]
+    if len(parts) != 3:
+        raise ValueError(f"bad vector {s!r}")
+    return parts
+
+
+def _val(el, units: str, conv=float):
+    got = el.get("units")
+    if got != units:
+        raise ValueError(f"invalid units for {el.tag}: expected {units!r}, got {got!r}")
+    return conv(el.get("value"))
+
+
+class Units:
+    def __init__(self, dt: float, dx: float, origin):
+        self.dx, self.dt = dx, dt
+        self.mass = BLOOD_DENSITY * dx * dx * dx
+        self.speed = dx / dt
+        self.pressure = self.mass / (dx * dt * dt)
+
+    def pressure_to_lattice(self, p_mmhg: float) -> float:
+        return CS2 + self.pressure_diff_to_lattice(p_mmhg - REFERENCE_PRESSURE_MMHG)
+
+    def pressure_diff_to_lattice(self, dp: float) -> float:
+        return dp * MMHG_TO_PASCAL / self.pressure
+
+    def to_lattice(self, units: str, value: float) -> float:
+        if units == "m":
+            sf = self.dx
+        elif units == "s":
+            sf = self.dt
+        elif units in ("rad", "dimensionless"):
+            sf = 1.0
+        elif units == "m/s":
+            sf = self.dx / self.dt
+        elif units == "mmHg":
+            sf = self.mass / (self.dx * self.dt * self.dt) / MMHG_TO_PASCAL
+        else:
+            raise ValueError(units)
+        return value / sf
+
+    def resistance(self, r: float) -> float:
+        return r * ((self.dt * self.dx) / BLOOD_DENSITY)
+
+    def capacitance(self, c: float) -> float:
+        return c * (BLOOD_DENSITY / (self.dt * self.dt * self.dx))
+
+    def area(self, a: float) -> float:
+        return a / (self.dx * self.dx)
+
+
+@dataclass
+class IoletCfg:
+    kind: str                  # "cosine", "wk3", "parabolic"
+    position: List[float]
+    normal: List[float]
+    density_mean: float = 0.0
+    density_amp: float = 0.0
+    phase: float = 0.0
+    period: float = 1.0
+    warmup: int = 0
+    radius: float = 0.0
+    max_speed: float = 0.0
+    rc: float = 0.0
+    rp: float = 0.0
+    cp: float = 0.0
+    area: float = 0.0
+
+
+@dataclass
+class CaseCfg:
+    gmy_path: str
+    tau: float
+    total_steps: int
+    warmup: int
+    initial_density: float
+    initial_step: int
+    relaxation_parameter: float
+    viscosity_ratio: float
+    sponge_width: float
+    sponge_lifetime: int
+    inlets: List[IoletCfg] = field(default_factory=list)
+    outlets: List[IoletCfg] = field(default_factory=list)
+    dt: float = 0.0
+    dx: float = 0.0
+
+
+def _normalised(v):
+    m2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2]
+    if v == [0.0, 0.0, 0.0]:
+        return v
+    m = math.sqrt(m2)
+    return [v[0] / m, v[1] / m, v[2] / m]
+
+
+def load_case(xml_path: str, kernel: str = "LBGK") -> CaseCfg:
+    root = ET.parse(xml_path).getroot()
+    if root.tag != "hemelbsettings" or root.get("version") != "3":
+        raise ValueError("not a version-3 hemelbsettings file")
+    sim = root.find("simulation")
+    steps = _val(sim.find("steps"), "lattice", int)
+    dt = _val(sim.find("step_length"), "s")
+    wu_el = sim.find("extra_warmup_steps")
+    warmup = 0
+    if wu_el is not None:
+        warmup = _val(wu_el, "lattice", int)
+        steps += warmup
+    relax = 0.0
+    if kernel in ("TRT",):
+        relax = _val(sim.find("relaxation_parameter"), "lattice")
+    dx = _val(sim.find("voxel_size"), "m")
+    origin = _vec(sim.find("origin").get("value"))
+    u = Units(dt, dx, origin)
+    tau = 0.5 + (dt * BLOOD_VISCOSITY / BLOOD_DENSITY) / (CS2 * dx * dx)
+    gmy = root.find("geometry").find("datafile").get("path")
+    gmy = os.path.join(os.path.dirname(os.path.abspath(xml_path)), gmy)
+
+    ic = root.find("initialconditions")
+    t0 = 0
+    tel = ic.find("time")
+    if tel is not None:
+        t0 = _val(tel, "lattice", int)
+    p0 = _val(ic.find("pressure").find("uniform"), "mmHg")
+    rho0 = u.pressure_to_lattice(p0) / CS2
+    vr = sw = 0.0
+    life = 0
+    if kernel == "LBGKLESSL":
+        sp = ic.find("sponge_layer")
+        vr = _val(sp.find("viscosity_ratio"), "dimensionless")
+        sw = u.to_lattice("m", _val(sp.find("width"), "m"))
+        life = _val(sp.find("lifetime"), "lattice", int)
+
+    def iolets(group: str) -> List[IoletCfg]:
+        out = []
+        for el in root.find(group).findall(group[:-1]):
+            cond = el.find("condition")
+            pos = _vec(el.find("position").get("value"))
+            if el.find("position").get("units") != "lattice":
+                raise ValueError("iolet position must be in lattice units")
+            nrm = _normalised(_vec(el.find("normal").get("value")))
+            typ, sub = cond.get("type"), cond.get("subtype")
+            if typ == "pressure" and sub == "cosine":
+                io = IoletCfg("cosine", pos, nrm)
+                io.density_amp = u.pressure_diff_to_lattice(_val(cond.find("amplitude"), "mmHg")) / CS2
+                io.density_mean = u.pressure_to_lattice(_val(cond.find("mean"), "mmHg")) / CS2
+                io.phase = u.to_lattice("rad", _val(cond.find("phase"), "rad"))
+                io.period = u.to_lattice("s", _val(cond.find("period"), "s"))
+                io.warmup = warmup
+            elif typ == "pressure" and sub == "WK3":
+                io = IoletCfg("wk3", pos, nrm)
+                io.rc = u.resistance(_val(cond.find("Rc"), "kg/m^4*s"))
+                io.rp = u.resistance(_val(cond.find("Rp"), "kg/m^4*s"))
+                io.cp = u.capacitance(_val(cond.find("Cp"), "m^4*s^2/kg"))
+                io.radius = u.to_lattice("m", _val(cond.find("radius"), "m"))
+                io.area = u.area(_val(cond.find("area"), "m^2"))
+            elif typ == "velocity" and sub == "parabolic":
+                io = IoletCfg("parabolic", pos, nrm)
+                io.radius = u.to_lattice("m", _val(cond.find("radius"), "m"))
+                io.max_speed = u.to_lattice("m/s", _val(cond.find("maximum"), "m/s"))
+                io.warmup = warmup
+            else:
+                raise ValueError(f"unsupported iolet condition {typ}/{sub}")
+            out.append(io)
+        return out
+
+    return CaseCfg(gmy_path=gmy, tau=tau, total_steps=steps, warmup=warmup, initial_density=rho0,
+                   initial_step=t0 if t0 else 1, relaxation_parameter=relax, viscosity_ratio=vr,
+                   sponge_width=sw, sponge_lifetime=life, inlets=iolets("inlets"),
+                   outlets=iolets("outlets"), dt=dt, dx=dx)
