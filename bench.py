@@ -1,0 +1,276 @@
+"""Benchmark: D3Q19 collide-and-stream on the 4M-site pipe, FP64 plain form.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
+
+A step is one time step over the whole lattice.  The default workload is the
+large straight pipe (radius 40, length 800, 4,019,200 fluid sites; LBGK
+tau=0.55, BFL walls, parabolic inlet ramped over 1000 steps, Nash pressure
+outlet), generated synthetically with the same shapes as the reference's
+configuration.  With N > 1 (torchrun), every rank runs its own replica: the
+plain form does not shard, so there is no collective on the data path.
+
+Rank 0 prints one JSON line.  `value` is whole-job MLUPS (site updates per
+second over all ranks / 1e6) timed with CUDA events on the library's stream,
+max over ranks; `e2e` is the same metric measured through the C ABI one
+hb_step call at a time (each call uploads the step's iolet densities and
+reads back the stability word, with a host synchronisation).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS & % HBM roofline, FP64 plain vs mixed/batched; p50/p99 solve latency"
+WORKLOADS = {
+    # name: (description, kernel, wall, algorithmic bytes per site update)
+    "pipe_r40": ("straight rigid pipe r=40 L=800 (4,019,200 sites), LBGK tau=0.55, BFL walls, parabolic inlet "
+                 "u=0.02 ramped over 1000 steps, Nash pressure outlet rho=1, FP64 plain", "LBGK", "BFL", 304),
+    "pipe_r40_short": ("straight rigid pipe r=40 L=200 (1,004,800 sites), same physics as pipe_r40; the case "
+                       "the kernel profiles capture", "LBGK", "BFL", 304),
+    "pipe_r8": ("straight rigid pipe r=8 L=64 (13,312 sites), LBGK tau=0.8, bounce-back walls, Nash pressure "
+                "iolets rho 1.001/0.999, FP64 plain", "LBGK", "SBB", 304),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(name: str, out_dir: str):
+    from hemepure_b200 import vessels
+    xml, gmy, info = vessels.make_case(name, out_dir)
+    return xml, info
+
+
+def cpu_baseline(xml: str, kernel: str, wall: str, n_sites: int, budget_s: float = 12.0, threads: int = 0):
+    """The oracle (the reference's algorithm restated in C) on the host cores."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    sim = O.Simulation(xml, kernel, wall, threads=threads)
+    t0 = time.perf_counter()
+    sim.run(1)
+    one = time.perf_counter() - t0
+    steps = max(1, int(budget_s / max(one, 1e-6)))
+    t0 = time.perf_counter()
+    rc = sim.run(steps)
+    dt = time.perf_counter() - t0
+    return {"value": n_sites * steps / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": f"{steps} full time steps of the same lattice after 1 warm-up step "
+                      f"({n_sites * steps} site updates, {dt:.1f} s, {threads} threads, status {rc})"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="pipe_r40", choices=sorted(WORKLOADS))
+    ap.add_argument("--case-dir", default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    desc, kernel, wall, bytes_per_site = WORKLOADS[args.workload]
+    warmup = max(3, args.warmup)
+
+    case_root = args.case_dir or os.path.join(tempfile.gettempdir(), f"hemeb200_bench_{os.getuid()}")
+    case_dir = os.path.join(case_root, f"{args.workload}_rank{rank}")
+    xml, info = make_workload(args.workload, case_dir)
+    n_sites = info.fluid_sites
+    config = {"workload": args.workload + ": " + desc, "sites": n_sites, "kernel": kernel, "wall": wall,
+              "storage": "fp64", "l2": "inputs larger than L2: two 19-plane FP64 buffers of %.2f GB each"
+              % (19 * n_sites * 8 / 1e9), "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # The reference itself cannot be built here (it needs MPI, Boost and ParMETIS,
+        # which are absent); its algorithm runs as the C restatement on all host threads.
+        total_budget = 150.0
+        from oracle import oracle as O
+        threads = os.cpu_count() or 1
+        sim = O.Simulation(xml, kernel, wall, threads=threads)
+        t0 = time.perf_counter()
+        sim.run(1)
+        one = time.perf_counter() - t0
+        steps = int(max(1, min(args.steps, total_budget / max(one, 1e-6))))
+        t0 = time.perf_counter()
+        sim.run(steps)
+        dt = time.perf_counter() - t0
+        v = n_sites * steps / dt / 1e6
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": warmup, "ms_per_step": dt * 1e3 / steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": threads, "kind": "port",
+                                 "sample": f"{steps} of {args.steps} requested time steps (bounded to ~{total_budget:.0f} s) "
+                                           f"of the full lattice after 1 warm-up step"},
+                "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_mod
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from hemepure_b200 import lbm
+
+    sim = lbm.LBM(xml, kernel=kernel, wall=wall, device=local)
+    sim.step(warmup)
+
+    # Timed region: K steps, CUDA events on the library's stream.
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.step(args.steps)
+    wall_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    ms, launches = sim.last_step_timing()
+    clocks = sampler.stop()
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n_sites * args.steps / (ms * 1e-3) / 1e6
+
+    # Roofline of the dominant kernel: per-launch CUDA events (serialised launches).
+    prof_steps = 200
+    b_ms, g_ms, w_ms = sim.profile_steps(prof_steps)
+    from hemepure_b200.lbm import Geometry, read_case
+    p, gmy = read_case(xml, kernel)
+    lay = Geometry(gmy).layout(p, wall)
+    bulk_launch_ms = b_ms / prof_steps
+    achieved = bytes_per_site * lay["bulk_sites"] / (bulk_launch_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as fh:
+            tj = json.load(fh)
+        if tj.get("workload") == args.workload:
+            traffic = tj.get("bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "k_bulk (plain bulk sites)", "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": bytes_per_site * lay["bulk_sites"],
+                "launch_ms": bulk_launch_ms, "boundary_launch_ms": g_ms / prof_steps,
+                "whole_step_frac": (bytes_per_site * n_sites / (ms / args.steps * 1e-3) / 1e9) / peak}
+
+    # End to end through the C ABI: one hb_step call per step, host-synchronised.
+    e2e_steps = min(args.steps, 500)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.step(1)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * n_sites * e2e_steps / e2e_s / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": 32 * 8,
+           "d2h_bytes_per_step": 4, "steps": e2e_steps,
+           "note": "one hb_step(1) call per step: iolet densities up, stability word down, host sync"}
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(xml, kernel, wall, n_sites)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+                "warmup": warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "clocks": clocks,
+                "gpu_launches": int(launches), "wall_s": wall_s}
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

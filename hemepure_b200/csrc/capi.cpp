@@ -1,0 +1,341 @@
+// capi.cpp -- the extern "C" boundary (include/hemeb200.h).  No C++ exception
+// crosses it: every entry point catches and returns an HB_* status.
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/hemeb200.h"
+#include "config.h"
+#include "extraction.h"
+#include "solver.h"
+
+struct hb_handle {
+  std::unique_ptr<hb::Solver> solver;
+  std::string error;
+};
+
+struct hb_geometry {
+  hb::LatticeTables tables;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <class F>
+int guard(hb_handle* h, F&& fn) {
+  try {
+    return fn();
+  } catch (const hb::Error& e) {
+    if (h) h->error = e.msg;
+    else g_create_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    if (h) h->error = "host memory exhausted";
+    else g_create_error = "host memory exhausted";
+    return HB_ERR_OOM;
+  } catch (const std::exception& e) {
+    if (h) h->error = e.what();
+    else g_create_error = e.what();
+    return HB_ERR_ARG;
+  }
+}
+
+int finish_create(hb::LatticeTables t, const hb_params& p, const hb_options& o, hb_handle** out) {
+  auto h = std::make_unique<hb_handle>();
+  h->solver = std::make_unique<hb::Solver>(std::move(t), p, o);
+  *out = h.release();
+  return HB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void hb_default_options(hb_options* opt) {
+  if (!opt) return;
+  opt->kernel = HB_KERNEL_LBGK;
+  opt->wall = HB_WALL_SBB;
+  opt->precision = HB_STORE_FP64;
+  opt->device = 0;
+}
+
+int hb_create_from_xml(const char* xml_path, const hb_options* opt, hb_handle** out) {
+  if (!xml_path || !out) return HB_ERR_ARG;
+  *out = nullptr;
+  return guard(nullptr, [&] {
+    hb_options o;
+    hb_default_options(&o);
+    if (opt) o = *opt;
+    hb::CaseConfig c = hb::read_case(xml_path, o.kernel);
+    hb::LatticeTables t = hb::read_gmy(c.gmy_path);
+    int rc = finish_create(std::move(t), c.params, o, out);
+    if (rc == HB_OK) (*out)->solver->set_units(c.dt, c.dx, c.origin);
+    if (rc == HB_OK && !c.checkpoint_file.empty()) {
+      std::string cp = c.checkpoint_file;
+      if (!cp.empty() && cp[0] != '/') {
+        std::string xp(xml_path);
+        size_t sl = xp.rfind('/');
+        if (sl != std::string::npos) cp = xp.substr(0, sl + 1) + cp;
+      }
+      try {
+        hb::read_checkpoint(*(*out)->solver, cp, c.has_time ? c.params.initial_step : 0);
+      } catch (...) {
+        delete *out;
+        *out = nullptr;
+        throw;
+      }
+    }
+    return rc;
+  });
+}
+
+int hb_create(const hb_lattice_desc* lat, const hb_params* params, const hb_options* opt, hb_handle** out) {
+  if (!lat || !params || !out || lat->n_sites <= 0 || !lat->coords || !lat->wall_mask || !lat->iolet_mask ||
+      !lat->site_type || !lat->iolet_id)
+    return HB_ERR_ARG;
+  *out = nullptr;
+  return guard(nullptr, [&] {
+    hb_options o;
+    hb_default_options(&o);
+    if (opt) o = *opt;
+    hb::LatticeTables t;
+    const int64_t n = lat->n_sites;
+    t.n = n;
+    for (int d = 0; d < 3; d++) t.dims[d] = lat->dims[d];
+    t.coords.assign(lat->coords, lat->coords + 3 * n);
+    t.wall.assign(lat->wall_mask, lat->wall_mask + n);
+    t.iolet.assign(lat->iolet_mask, lat->iolet_mask + n);
+    t.stype.assign(lat->site_type, lat->site_type + n);
+    t.iolet_id.assign(lat->iolet_id, lat->iolet_id + n);
+    if (lat->wall_distance) t.q.assign(lat->wall_distance, lat->wall_distance + 18 * n);
+    if (lat->wall_normal) t.normal.assign(lat->wall_normal, lat->wall_normal + 3 * n);
+    else t.normal.assign(3 * n, 0.0);
+    for (int64_t i = 0; i < n; i++) t.type_counts[t.collision_type(i)]++;
+    if (lat->neighbours) {
+      t.nbr.assign(lat->neighbours, lat->neighbours + 19 * n);
+    } else {
+      hb::build_neighbours(t);
+    }
+    return finish_create(std::move(t), *params, o, out);
+  });
+}
+
+int hb_destroy(hb_handle* h) {
+  if (!h) return HB_ERR_ARG;
+  delete h;
+  return HB_OK;
+}
+
+int hb_last_error(const hb_handle* h, char* msg, size_t len) {
+  if (!msg || len == 0) return HB_ERR_ARG;
+  const std::string& e = h ? h->error : g_create_error;
+  std::strncpy(msg, e.c_str(), len - 1);
+  msg[len - 1] = '\0';
+  return HB_OK;
+}
+
+int hb_request_comms(hb_handle* h) {
+  if (!h) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->request_comms();
+    return HB_OK;
+  });
+}
+
+int hb_pre_send(hb_handle* h) { return h ? HB_OK : HB_ERR_ARG; }
+
+int hb_pre_receive(hb_handle* h, uint32_t flags) {
+  if (!h) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->pre_receive((flags & HB_STEP_MACRO) != 0);
+    return HB_OK;
+  });
+}
+
+int hb_post_receive(hb_handle* h) { return h ? HB_OK : HB_ERR_ARG; }
+
+int hb_end_iteration(hb_handle* h) {
+  if (!h) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->end_iteration();
+    const int st = h->solver->read_status();
+    if (st & hb::kStatusIoletRadius) return HB_ERR_IOLET_RADIUS;
+    if (st & hb::kStatusUnstable) return HB_UNSTABLE;
+    return HB_OK;
+  });
+}
+
+int hb_step(hb_handle* h, int64_t n_steps, uint32_t flags) {
+  if (!h) return HB_ERR_ARG;
+  return guard(h, [&] { return h->solver->step(n_steps, flags); });
+}
+
+int hb_site_count(const hb_handle* h, int64_t* n) {
+  if (!h || !n) return HB_ERR_ARG;
+  *n = h->solver->tables().n;
+  return HB_OK;
+}
+
+int hb_time_step(const hb_handle* h, uint64_t* t) {
+  if (!h || !t) return HB_ERR_ARG;
+  *t = h->solver->time_step();
+  return HB_OK;
+}
+
+int hb_get_params(const hb_handle* h, hb_params* p) {
+  if (!h || !p) return HB_ERR_ARG;
+  *p = h->solver->params();
+  return HB_OK;
+}
+
+int hb_get_fs(hb_handle* h, double* f) {
+  if (!h || !f) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->get_fs(f);
+    return HB_OK;
+  });
+}
+
+int hb_set_fs(hb_handle* h, const double* f) {
+  if (!h || !f) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->set_fs(f);
+    return HB_OK;
+  });
+}
+
+int hb_get_macro(hb_handle* h, double* density, double* velocity, double* wss) {
+  if (!h) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->get_macro(density, velocity, wss);
+    return HB_OK;
+  });
+}
+
+int hb_get_wk3(hb_handle* h, int group, int index, double state[4]) {
+  if (!h || !state || group < 0 || group > 1 || index < 0 || index > 15) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->get_wk3(group, index, state);
+    return HB_OK;
+  });
+}
+
+int hb_get_tables(const hb_handle* h, int64_t* neighbours, uint32_t* wall_mask, uint32_t* iolet_mask, int32_t* site_type,
+                  int32_t* iolet_id, int64_t* coords, int64_t* type_counts) {
+  if (!h) return HB_ERR_ARG;
+  const hb::LatticeTables& t = h->solver->tables();
+  const size_t n = (size_t)t.n;
+  if (neighbours) std::memcpy(neighbours, t.nbr.data(), n * 19 * sizeof(int64_t));
+  if (wall_mask) std::memcpy(wall_mask, t.wall.data(), n * sizeof(uint32_t));
+  if (iolet_mask) std::memcpy(iolet_mask, t.iolet.data(), n * sizeof(uint32_t));
+  if (site_type) std::memcpy(site_type, t.stype.data(), n * sizeof(int32_t));
+  if (iolet_id) std::memcpy(iolet_id, t.iolet_id.data(), n * sizeof(int32_t));
+  if (coords) std::memcpy(coords, t.coords.data(), n * 3 * sizeof(int64_t));
+  if (type_counts) std::memcpy(type_counts, t.type_counts, 6 * sizeof(int64_t));
+  return HB_OK;
+}
+
+int hb_write_xtr(hb_handle* h, const char* path, const char* fields, const char* offset_path) {
+  if (!h || !path || !fields) return HB_ERR_ARG;
+  return guard(h, [&] {
+    hb::write_xtr(*h->solver, path, fields, offset_path ? offset_path : "");
+    return HB_OK;
+  });
+}
+
+int hb_read_checkpoint(hb_handle* h, const char* path, uint64_t step) {
+  if (!h || !path) return HB_ERR_ARG;
+  return guard(h, [&] {
+    hb::read_checkpoint(*h->solver, path, step);
+    return HB_OK;
+  });
+}
+
+int hb_read_case(const char* xml_path, int kernel, hb_params* params, char* gmy_path, size_t gmy_path_len) {
+  if (!xml_path || !params) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    hb::CaseConfig c = hb::read_case(xml_path, kernel);
+    *params = c.params;
+    if (gmy_path && gmy_path_len) {
+      std::strncpy(gmy_path, c.gmy_path.c_str(), gmy_path_len - 1);
+      gmy_path[gmy_path_len - 1] = '\0';
+    }
+    return HB_OK;
+  });
+}
+
+int hb_geometry_open(const char* gmy_path, hb_geometry** out) {
+  if (!gmy_path || !out) return HB_ERR_ARG;
+  *out = nullptr;
+  return guard(nullptr, [&] {
+    auto g = std::make_unique<hb_geometry>();
+    g->tables = hb::read_gmy(gmy_path);
+    *out = g.release();
+    return HB_OK;
+  });
+}
+
+int hb_geometry_site_count(const hb_geometry* g, int64_t* n, int64_t dims[3]) {
+  if (!g || !n) return HB_ERR_ARG;
+  *n = g->tables.n;
+  if (dims)
+    for (int d = 0; d < 3; d++) dims[d] = g->tables.dims[d];
+  return HB_OK;
+}
+
+int hb_geometry_tables(const hb_geometry* g, int64_t* neighbours, uint32_t* wall_mask, uint32_t* iolet_mask,
+                       int32_t* site_type, int32_t* iolet_id, int64_t* coords, int64_t* type_counts,
+                       double* wall_distance, double* wall_normal) {
+  if (!g) return HB_ERR_ARG;
+  const hb::LatticeTables& t = g->tables;
+  const size_t n = (size_t)t.n;
+  if (neighbours) std::memcpy(neighbours, t.nbr.data(), n * 19 * sizeof(int64_t));
+  if (wall_mask) std::memcpy(wall_mask, t.wall.data(), n * sizeof(uint32_t));
+  if (iolet_mask) std::memcpy(iolet_mask, t.iolet.data(), n * sizeof(uint32_t));
+  if (site_type) std::memcpy(site_type, t.stype.data(), n * sizeof(int32_t));
+  if (iolet_id) std::memcpy(iolet_id, t.iolet_id.data(), n * sizeof(int32_t));
+  if (coords) std::memcpy(coords, t.coords.data(), n * 3 * sizeof(int64_t));
+  if (type_counts) std::memcpy(type_counts, t.type_counts, 6 * sizeof(int64_t));
+  if (wall_distance) std::memcpy(wall_distance, t.q.data(), n * 18 * sizeof(double));
+  if (wall_normal) std::memcpy(wall_normal, t.normal.data(), n * 3 * sizeof(double));
+  return HB_OK;
+}
+
+int hb_geometry_layout(const hb_geometry* g, const hb_params* params, int wall, int64_t stats[4]) {
+  if (!g || !params || !stats) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    hb::Layout L = hb::build_layout(g->tables, *params, wall);
+    stats[0] = L.axis;
+    stats[1] = L.runs;
+    stats[2] = L.bulk_sites;
+    stats[3] = L.G;
+    return HB_OK;
+  });
+}
+
+int hb_geometry_close(hb_geometry* g) {
+  if (!g) return HB_ERR_ARG;
+  delete g;
+  return HB_OK;
+}
+
+int hb_last_step_timing(const hb_handle* h, double* ms, int64_t* launches) {
+  if (!h) return HB_ERR_ARG;
+  if (ms) *ms = h->solver->last_ms();
+  if (launches) *launches = h->solver->last_launches();
+  return HB_OK;
+}
+
+int hb_profile_steps(hb_handle* h, int64_t n_steps, double ms[3]) {
+  if (!h || !ms || n_steps < 0) return HB_ERR_ARG;
+  return guard(h, [&] { return h->solver->profile(n_steps, ms); });
+}
+
+int hb_device_bytes(const hb_handle* h, int64_t* bytes) {
+  if (!h || !bytes) return HB_ERR_ARG;
+  *bytes = h->solver->device_bytes();
+  return HB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,67 @@
+// config.h -- case-file reader (the reference's configuration::SimConfig) and the
+// lattice tables of one rank (the reference's geometry::LatticeData).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/hemeb200.h"
+#include "hb_common.h"
+
+namespace hb {
+
+// What SimConfig::DoIO extracts for the collide-and-stream path, converted to
+// lattice units by the reference's UnitConverter (src/util/UnitConverter.cc:15-118).
+struct CaseConfig {
+  std::string gmy_path;
+  double dt = 0, dx = 0;
+  double origin[3] = {0, 0, 0};
+  uint64_t total_steps = 0;       // <steps> + <extra_warmup_steps>
+  uint64_t warmup = 0;
+  hb_params params{};
+  struct PropertyOutput {
+    std::string file;
+    uint64_t period = 0;
+    std::string geometry;
+    std::vector<std::string> fields;
+  };
+  std::vector<PropertyOutput> outputs;
+  std::string checkpoint_file;    // <initialconditions><checkpoint file=...>
+  bool has_time = false;          // <initialconditions><time> present
+};
+
+// SimConfig::New + DoIO (src/configuration/SimConfig.cc:41-121).  `kernel` decides
+// which kernel-specific elements are required, as HEMELB_KERNEL does.
+CaseConfig read_case(const std::string& xml_path, int kernel);
+
+// Lattice tables in the reference's contiguous order
+// (src/geometry/LatticeData.cc:69-285, 366-443; LatticeData.h:375-436).
+struct LatticeTables {
+  int64_t n = 0;
+  int64_t dims[3] = {0, 0, 0};
+  int64_t block_size = 0;
+  int64_t blocks[3] = {0, 0, 0};
+  int64_t type_counts[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<int64_t> coords;      // [n*3]
+  std::vector<uint32_t> wall;       // [n]
+  std::vector<uint32_t> iolet;      // [n]
+  std::vector<int32_t> stype;       // [n] 0 fluid 1 inlet 2 outlet
+  std::vector<int32_t> iolet_id;    // [n]
+  std::vector<double> q;            // [n*18]
+  std::vector<double> normal;       // [n*3]
+  std::vector<int64_t> nbr;         // [n*19]
+
+  int collision_type(int64_t i) const {
+    const bool w = wall[i] != 0;
+    const int st = stype[i];
+    return !w ? (st == 0 ? 0 : (st == 1 ? 2 : 3)) : (st == 0 ? 1 : (st == 1 ? 4 : 5));
+  }
+};
+
+// GeometryReader::LoadAndDecompose on one rank + LatticeData construction.
+LatticeTables read_gmy(const std::string& path);
+// neighbourIndices from coordinates (LatticeData::InitialiseNeighbourLookup).
+void build_neighbours(LatticeTables& t);
+
+}  // namespace hb

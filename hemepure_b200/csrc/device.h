@@ -1,0 +1,91 @@
+// device.h -- device-side data layout shared by the host driver and the kernels.
+//
+// Layout in HBM (one lattice):
+//   f_a, f_b   [19][np] distributions, structure of arrays, ping-pong.  After a
+//              step the output buffer holds POST-collision values f*(x) (pull
+//              form); before the first step it holds PRE-collision f (direct form).
+//   meta       [n]  run id of a plain bulk site, or -(g+1) for general site g.
+//   run_off    [runs][20] per-direction source offset of a plain bulk site:
+//              slot i of site s is pulled from f*[i][s + run_off[run][i]].
+//   general    per general site (wall, iolet, or bulk sites whose neighbours do
+//              not follow the run pattern), structure of arrays, binned by
+//              collision type so a warp runs one streamer.
+#pragma once
+
+#include <cstdint>
+
+namespace hb {
+
+struct IoletDev {
+  int kind;               // IoletKind
+  int dir0;               // direction closest to the iolet normal
+  int wk3;                // index into the Windkessel state, or -1
+  int pad;
+  double pos[3];
+  double nrm[3];          // normalised normal (double)
+  double nrm_f[3];        // the normal narrowed to float and widened back (Nash ghost)
+  double radius, max_speed;
+  uint64_t warmup;
+};
+
+struct WK3Dev {           // InOutLetWK3 state
+  double density, density_new, flow, flow_old;
+  double rc, rp, cp, area;
+  int cpl_start, cpl_count;   // coupling slots of this iolet
+  int count_prev;             // coupling sites summed at the previous step (0 before the first)
+  int centre_couples;         // the centre site takes part in the coupling
+  int iolet;                  // index into the iolet table
+  int pad[3];
+};
+
+struct GeneralDev {
+  int G;
+  const int* site;        // [G] storage index
+  const uint32_t* wall;   // [G] wall-link mask (bit d-1 for direction d)
+  const uint32_t* iolet;  // [G] iolet-link mask
+  const int* src;         // [18][G] pull source of slots 1..18 (own index for boundary slots)
+  const float* q;         // [18][G] wall distances (BFL, GZS)
+  const float* nrm;       // [3][G] wall normal (float, normalised in float)
+  const int* io;          // [G] iolet table index or -1
+  const int* cpl;         // [G] Windkessel coupling slot or -1
+  const int* xyz;         // [3][G] global coordinates
+};
+
+struct StepArgs {
+  const double* fin;
+  double* fout;
+  int64_t np;
+  int n;
+  const int* meta;
+  const int* run_off;
+  GeneralDev gen;
+  // kernel parameters
+  double tau, omega, omega_minus;
+  const double* vtau;     // LES sponge tau per site (storage order) or null
+  uint64_t t;             // 1-based time step of this step
+  uint64_t lifetime;      // LES sponge lifetime
+  const IoletDev* iolets;
+  const double* dens_row; // iolet densities for this step [32]
+  double* cpl_buf;        // Windkessel coupling contributions
+  double* rho;            // macroscopic outputs in storage order (or null)
+  double* u;              // [3][np]
+  double* wss;
+  int* status;            // bit 0 unstable, bit 1 iolet radius, bit 2 bad neighbour
+};
+
+enum StatusBits { kStatusUnstable = 1, kStatusIoletRadius = 2, kStatusBadNeighbour = 4 };
+
+// Launchers (kernels_f64.cu).
+// `which`: 1 = plain bulk sites, 2 = general sites, 3 = both.
+void launch_step_f64(const StepArgs& a, int kernel, int wall, bool gather, bool macro, int which, int bulk_block,
+                     int general_block, void* stream);
+void launch_gather_f64(const StepArgs& a, int wall, void* stream);
+// Gather the pre-collision f straight into AoS reference order.
+void launch_gather_aos_f64(const StepArgs& a, int wall, const int* st2ref, double* aos, void* stream);
+void launch_wk3_begin(WK3Dev* wk3, int nwk3, const double* cpl_buf, double* dens_row, void* stream);
+void launch_equilibrium_f64(double* f, int64_t np, int n, const double feq[19], void* stream);
+// AoS reference order <-> SoA storage order.
+void launch_soa_to_aos_f64(const double* soa, int64_t np, const int* st2ref, int n, double* aos, void* stream);
+void launch_aos_to_soa_f64(const double* aos, const int* st2ref, int n, double* soa, int64_t np, void* stream);
+
+}  // namespace hb

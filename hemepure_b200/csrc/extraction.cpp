@@ -1,0 +1,290 @@
+// extraction.cpp -- .xtr v4 output, .off v1 offsets and checkpoint restore.
+//
+// Format (src/extraction/LocalPropertyOutput.cc:100-180, 217-365,
+// src/io/formats/extraction.h, src/io/formats/offset.h), all XDR big-endian:
+//   main header (60 B): hlb magic, 0x78747204, version 4, f64 voxel size,
+//     3 x f64 origin, u64 site count, u32 field count, u32 field-header length;
+//   per field: XDR string name, u32 floats per site, f64 offset;
+//   per record: u64 time step, then per site in contiguous order u32 x, y, z and
+//     the fields as f32 (pressure in mmHg minus the reference pressure, velocity
+//     in m/s, shear stress in Pa, distributions in lattice units).
+// A record labelled t carries the density/velocity/stress computed in step t and
+// the distributions that entered step t (GetFNew after the swap,
+// src/extraction/LbDataSourceIterator.cc:90-93).  The .off file holds the start
+// of the first record and its end.
+// Restore: src/extraction/LocalDistributionInput.cc:48-170 (binary search on the
+// record labels, float values plus the field offset into f_old and f_new).
+#include "extraction.h"
+
+#include <sys/stat.h>
+
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <vector>
+
+#include "../../include/hemeb200.h"
+#include "hb_common.h"
+#include "solver.h"
+
+namespace hb {
+
+namespace {
+
+constexpr uint32_t kHlbMagic = 0x686c6221u;
+constexpr uint32_t kXtrMagic = 0x78747204u;
+constexpr uint32_t kOffMagic = 0x6f666604u;
+constexpr double kMmHgToPascal = 133.3223874;
+
+struct XdrOut {
+  std::vector<unsigned char> b;
+  void u32(uint32_t v) {
+    for (int k = 3; k >= 0; k--) b.push_back((unsigned char)(v >> (8 * k)));
+  }
+  void u64(uint64_t v) {
+    u32((uint32_t)(v >> 32));
+    u32((uint32_t)v);
+  }
+  void f32(float f) {
+    uint32_t v;
+    std::memcpy(&v, &f, 4);
+    u32(v);
+  }
+  void f64(double d) {
+    uint64_t v;
+    std::memcpy(&v, &d, 8);
+    u64(v);
+  }
+  void str(const std::string& s) {
+    u32((uint32_t)s.size());
+    for (char c : s) b.push_back((unsigned char)c);
+    while (b.size() % 4) b.push_back(0);
+  }
+};
+
+struct XdrIn {
+  const unsigned char* p;
+  size_t n, pos = 0;
+  uint32_t u32() {
+    if (pos + 4 > n) throw Error{HB_ERR_FORMAT, "truncated XDR data"};
+    uint32_t v = (uint32_t(p[pos]) << 24) | (uint32_t(p[pos + 1]) << 16) | (uint32_t(p[pos + 2]) << 8) | uint32_t(p[pos + 3]);
+    pos += 4;
+    return v;
+  }
+  uint64_t u64() {
+    uint64_t hi = u32();
+    return (hi << 32) | u32();
+  }
+  float f32() {
+    uint32_t v = u32();
+    float f;
+    std::memcpy(&f, &v, 4);
+    return f;
+  }
+  double f64() {
+    uint64_t v = u64();
+    double d;
+    std::memcpy(&d, &v, 8);
+    return d;
+  }
+  std::string str() {
+    uint32_t len = u32();
+    if (pos + len > n) throw Error{HB_ERR_FORMAT, "truncated XDR string"};
+    std::string s((const char*)p + pos, len);
+    pos += len;
+    while (pos % 4) pos++;
+    return s;
+  }
+};
+
+std::vector<std::string> split_fields(const std::string& s) {
+  std::vector<std::string> out;
+  std::stringstream ss(s);
+  std::string item;
+  while (std::getline(ss, item, ',')) {
+    size_t a = item.find_first_not_of(" \t"), b = item.find_last_not_of(" \t");
+    if (a == std::string::npos) continue;
+    item = item.substr(a, b - a + 1);
+    if (item != "velocity" && item != "pressure" && item != "shearstress" && item != "distributions")
+      throw Error{HB_ERR_ARG, "Unrecognised field type '" + item + "'"};
+    out.push_back(item);
+  }
+  if (out.empty()) throw Error{HB_ERR_ARG, "no output fields"};
+  return out;
+}
+
+uint32_t field_len(const std::string& f) { return f == "velocity" ? 3u : (f == "distributions" ? 19u : 1u); }
+
+std::vector<unsigned char> read_file(const std::string& path) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) throw Error{HB_ERR_IO, "cannot open " + path};
+  return std::vector<unsigned char>((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+}
+
+}  // namespace
+
+void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv, const std::string& offset_path) {
+  const std::vector<std::string> fields = split_fields(fields_csv);
+  const LatticeTables& t = s.tables();
+  const int64_t n = t.n;
+  if (s.time_step() <= 1) throw Error{HB_ERR_ARG, "no completed time step to write"};
+  const uint64_t label = s.time_step() - 1;
+  bool need_macro = false, need_f = false;
+  for (auto& f : fields) {
+    if (f == "distributions") need_f = true;
+    else need_macro = true;
+  }
+  std::vector<double> rho, u, wss, fd;
+  if (need_macro) {
+    if (!s.macro_valid()) throw Error{HB_ERR_ARG, "the last step did not fill the macroscopic caches (pass HB_STEP_MACRO)"};
+    rho.resize(n);
+    u.resize(3 * n);
+    wss.resize(n);
+    s.get_macro(rho.data(), u.data(), wss.data());
+  }
+  if (need_f) {
+    fd.resize((size_t)n * Q);
+    if (!s.get_previous_fs(fd.data())) throw Error{HB_ERR_ARG, "the distributions of the last step are no longer held"};
+  }
+
+  // Unit conversion (src/util/UnitConverter.cc, UnitConverter.h:61-119).
+  const double dx = s.dx(), dt = s.dt();
+  const double mass = 1000.0 * dx * dx * dx;
+  const double lattice_pressure = mass / (dx * dt * dt);
+  const double lattice_speed = dx / dt;
+
+  XdrOut hdr;
+  {
+    XdrOut fh;
+    for (auto& f : fields) {
+      fh.str(f);
+      fh.u32(field_len(f));
+      fh.f64(0.0);  // REFERENCE_PRESSURE_mmHg for pressure, 0 otherwise
+    }
+    hdr.u32(kHlbMagic);
+    hdr.u32(kXtrMagic);
+    hdr.u32(4);
+    hdr.f64(dx);
+    hdr.f64(s.origin()[0]);
+    hdr.f64(s.origin()[1]);
+    hdr.f64(s.origin()[2]);
+    hdr.u64((uint64_t)n);
+    hdr.u32((uint32_t)fields.size());
+    hdr.u32((uint32_t)fh.b.size());
+    hdr.b.insert(hdr.b.end(), fh.b.begin(), fh.b.end());
+  }
+  XdrOut rec;
+  rec.u64(label);
+  for (int64_t i = 0; i < n; i++) {
+    rec.u32((uint32_t)t.coords[3 * i]);
+    rec.u32((uint32_t)t.coords[3 * i + 1]);
+    rec.u32((uint32_t)t.coords[3 * i + 2]);
+    for (auto& f : fields) {
+      if (f == "pressure") {
+        const double p = rho[i] * kCs2;
+        rec.f32((float)(0.0 + (p - kCs2) * lattice_pressure / kMmHgToPascal - 0.0));
+      } else if (f == "velocity") {
+        rec.f32((float)(u[3 * i] * lattice_speed));
+        rec.f32((float)(u[3 * i + 1] * lattice_speed));
+        rec.f32((float)(u[3 * i + 2] * lattice_speed));
+      } else if (f == "shearstress") {
+        rec.f32((float)(wss[i] * lattice_pressure));
+      } else {
+        for (int k = 0; k < Q; k++) rec.f32((float)fd[(size_t)i * Q + k]);
+      }
+    }
+  }
+
+  struct stat sb;
+  const bool exists = stat(path.c_str(), &sb) == 0 && sb.st_size > 0;
+  if (exists) {
+    std::vector<unsigned char> old = read_file(path);
+    if (old.size() < hdr.b.size() || std::memcmp(old.data(), hdr.b.data(), hdr.b.size()) != 0)
+      throw Error{HB_ERR_FORMAT, "existing .xtr file has a different header"};
+    if ((old.size() - hdr.b.size()) % rec.b.size() != 0) throw Error{HB_ERR_FORMAT, "existing .xtr file has a partial record"};
+    std::ofstream out(path, std::ios::binary | std::ios::app);
+    out.write((const char*)rec.b.data(), (std::streamsize)rec.b.size());
+    if (!out) throw Error{HB_ERR_IO, "cannot append to " + path};
+  } else {
+    std::ofstream out(path, std::ios::binary | std::ios::trunc);
+    out.write((const char*)hdr.b.data(), (std::streamsize)hdr.b.size());
+    out.write((const char*)rec.b.data(), (std::streamsize)rec.b.size());
+    if (!out) throw Error{HB_ERR_IO, "cannot write " + path};
+  }
+  if (!offset_path.empty()) {
+    XdrOut off;
+    off.u32(kHlbMagic);
+    off.u32(kOffMagic);
+    off.u32(1);
+    off.u32(1);
+    off.u64((uint64_t)hdr.b.size());
+    off.u64((uint64_t)(hdr.b.size() + rec.b.size()));
+    std::ofstream out(offset_path, std::ios::binary | std::ios::trunc);
+    out.write((const char*)off.b.data(), (std::streamsize)off.b.size());
+    if (!out) throw Error{HB_ERR_IO, "cannot write " + offset_path};
+  }
+}
+
+void read_checkpoint(Solver& s, const std::string& path, uint64_t step) {
+  std::vector<unsigned char> buf = read_file(path);
+  XdrIn x{buf.data(), buf.size()};
+  if (x.u32() != kHlbMagic) throw Error{HB_ERR_FORMAT, "This file does not start with the HemeLB magic number."};
+  if (x.u32() != kXtrMagic) throw Error{HB_ERR_FORMAT, "This file is not an extraction file."};
+  if (x.u32() != 4) throw Error{HB_ERR_FORMAT, "Unsupported extraction version."};
+  x.f64();
+  x.f64();
+  x.f64();
+  x.f64();
+  const uint64_t nsites = x.u64();
+  const uint32_t nfields = x.u32();
+  const uint32_t fhl = x.u32();
+  (void)fhl;
+  if (nfields != 1) throw Error{HB_ERR_FORMAT, "a checkpoint holds exactly one field"};
+  const std::string name = x.str();
+  const uint32_t nf = x.u32();
+  const double offset = x.f64();
+  if (name != "distributions" || nf != (uint32_t)Q) throw Error{HB_ERR_FORMAT, "checkpoint field is not 'distributions' of 19 values"};
+  const LatticeTables& t = s.tables();
+  if ((int64_t)nsites != t.n) throw Error{HB_ERR_FORMAT, "checkpoint site count differs from the lattice"};
+  const size_t hdr = x.pos;
+  const size_t reclen = 8 + (size_t)nsites * (12 + 4 * Q);
+  if ((buf.size() - hdr) % reclen != 0) throw Error{HB_ERR_FORMAT, "Checkpoint file length not consistent with integer number of checkpoints"};
+  const size_t ntimes = (buf.size() - hdr) / reclen;
+  if (ntimes == 0) throw Error{HB_ERR_FORMAT, "checkpoint file holds no record"};
+  auto label_of = [&](size_t k) {
+    XdrIn r{buf.data() + hdr + k * reclen, 8};
+    return r.u64();
+  };
+  size_t idx = ntimes - 1;
+  if (step) {
+    size_t lo = 0, len = ntimes;
+    while (len) {
+      size_t half = len / 2, m = lo + half;
+      if (label_of(m) < step) {
+        lo = m + 1;
+        len -= half + 1;
+      } else {
+        len = half;
+      }
+    }
+    if (lo >= ntimes || label_of(lo) != step) throw Error{HB_ERR_ARG, "Target timestep not found in checkpoint file."};
+    idx = lo;
+  }
+  XdrIn r{buf.data() + hdr + idx * reclen, reclen};
+  const uint64_t label = r.u64();
+  std::vector<double> f((size_t)t.n * Q);
+  for (int64_t i = 0; i < t.n; i++) {
+    const uint32_t px = r.u32(), py = r.u32(), pz = r.u32();
+    if ((int64_t)px != t.coords[3 * i] || (int64_t)py != t.coords[3 * i + 1] || (int64_t)pz != t.coords[3 * i + 2])
+      throw Error{HB_ERR_FORMAT, "Site read at index " + std::to_string(i) + " does not match the lattice's site order"};
+    for (int k = 0; k < Q; k++) {
+      float v = r.f32();
+      v = (float)((double)v + offset);
+      f[(size_t)i * Q + k] = (double)v;
+    }
+  }
+  s.set_fs(f.data());
+  s.set_time_step(label);
+}
+
+}  // namespace hb

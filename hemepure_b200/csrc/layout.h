@@ -1,0 +1,48 @@
+// layout.h -- device layout of one lattice, built on the host from the
+// reference-order tables.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/hemeb200.h"
+#include "config.h"
+
+namespace hb {
+
+struct Layout {
+  int n = 0;
+  int64_t np = 0;                 // padded stride of one direction plane
+  int axis = 2;                   // run axis
+  std::vector<int> st2ref, ref2st;
+  std::vector<int> meta;          // [n]
+  std::vector<int> run_off;       // [runs*20]
+  int runs = 0;
+  int bulk_sites = 0;
+  // general sites (structure of arrays)
+  int G = 0;
+  std::vector<int> g_site, g_src, g_io, g_cpl, g_xyz, g_kind;
+  std::vector<uint32_t> g_wall, g_iolet;
+  std::vector<float> g_q, g_nrm;
+  int kind_start[7] = {0, 0, 0, 0, 0, 0, 0};   // bins by collision type
+  // Windkessel coupling slots (reference order within each iolet)
+  struct Coupling {
+    int iolet = -1;               // table index (inlets 0..15, outlets 16..31)
+    int start = 0, count = 0;
+    int centre_ref = -1;
+    bool centre_couples = false;
+  };
+  std::vector<Coupling> couplings; // one per WK3 iolet
+  int cpl_total = 0;
+  int dir0[32];
+};
+
+// Builds the layout; throws hb::Error (HB_ERR_UNSUPPORTED / HB_ERR_BAD_INDEX) for
+// lattices whose streaming pattern the pull form cannot reproduce exactly.
+Layout build_layout(const LatticeTables& t, const hb_params& p, int wall);
+
+// Direction closest to an iolet normal (SortDirectionsCloseToIOletNormal,
+// src/lb/streamers/NashZerothOrderPressureDelegate.h:95-116).
+int closest_direction(const double n[3]);
+
+}  // namespace hb

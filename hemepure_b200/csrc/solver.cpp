@@ -1,0 +1,482 @@
+// solver.cpp -- device state and the time-step loop of one lattice.
+//
+// One step (src/lb/lb.hpp:191-346 and src/SimulationMaster.cc:346-383):
+//   RequestComms   Windkessel DoComms on the device (k_wk3_begin), cosine
+//                  densities from the host table (InOutLetCosine::GetDensity with
+//                  the 0-indexed step, BoundaryValues.cc:211-214)
+//   PreReceive     k_bulk over plain bulk sites, k_general over the rest
+//   PostReceive    nothing: the BFL post-step is applied when the next step
+//                  gathers (kernels_f64.cu)
+//   EndIteration   swap the two buffers, time step + 1
+#include "solver.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace hb {
+
+DeviceBuffer::~DeviceBuffer() {
+  if (p) cudaFree(p);
+}
+
+void DeviceBuffer::alloc(size_t b) {
+  if (p) {
+    cudaFree(p);
+    p = nullptr;
+  }
+  bytes = b;
+  if (b == 0) return;
+  cudaError_t e = cudaMalloc(&p, b);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    throw Error{e == cudaErrorMemoryAllocation ? HB_ERR_OOM : HB_ERR_CUDA,
+                std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e)};
+  }
+}
+
+void Solver::check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error{HB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+namespace {
+
+// Lattice::CalculateFeq at zero momentum (the equilibrium initial condition,
+// src/lb/InitialCondition.hpp:29-40).
+void feq_host(double rho, double mx, double my, double mz, double* feq) {
+  const double th = (3. / 2.) * (mx * mx + my * my + mz * mz);
+  const double d1 = 1. / rho;
+  const double nh = (9. / 2.) * d1;
+  for (int i = 0; i < Q; i++) {
+    const double mde = (double)cx(i) * mx + (double)cy(i) * my + (double)cz(i) * mz;
+    const double t1 = rho - th * d1;
+    feq[i] = weight(i) * ((t1 + nh * (mde * mde)) + 3. * mde);
+  }
+}
+
+template <class T>
+void upload_vec(DeviceBuffer& b, const std::vector<T>& v, int64_t& total) {
+  b.alloc(v.size() * sizeof(T));
+  if (!v.empty()) {
+    cudaError_t e = cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) throw Error{HB_ERR_CUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(e)};
+  }
+  total += (int64_t)b.bytes;
+}
+
+}  // namespace
+
+Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& opt)
+    : t_(std::move(tables)), p_(params), opt_(opt) {
+  if (opt_.kernel < 0 || opt_.kernel > 2 || opt_.wall < 0 || opt_.wall > 2) throw Error{HB_ERR_ARG, "unknown kernel or wall type"};
+  if (opt_.precision != HB_STORE_FP64) throw Error{HB_ERR_UNSUPPORTED, "this handle type stores FP64 distributions"};
+  if (opt_.kernel == kLES && opt_.wall == kGZS)
+    throw Error{HB_ERR_UNSUPPORTED, "GZS walls with the LES kernel: the virtual-node collision has no relaxation time"};
+  if (!(p_.tau > 0.5)) throw Error{HB_ERR_ARG, "tau must exceed 1/2"};
+  for (int k = 0; k < p_.n_inlets + p_.n_outlets; k++) {
+    const hb_iolet& io = k < p_.n_inlets ? p_.inlets[k] : p_.outlets[k - p_.n_inlets];
+    if (io.kind < 0 || io.kind > 2) throw Error{HB_ERR_ARG, "unknown iolet kind"};
+  }
+  if ((opt_.wall == kBFL || opt_.wall == kGZS) && t_.q.empty()) throw Error{HB_ERR_ARG, "BFL and GZS walls need wall distances"};
+  check(cudaSetDevice(opt_.device), "cudaSetDevice");
+  L_ = build_layout(t_, p_, opt_.wall);
+  t_step_ = p_.initial_step ? p_.initial_step : 1;
+  omega_ = -1.0 / p_.tau;
+  {
+    const double lambda = p_.relaxation_parameter;
+    const double tau_minus = 0.5 + lambda / (p_.tau - 0.5);
+    omega_minus_ = -1.0 / tau_minus;
+  }
+  check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreate(&ev0_), "cudaEventCreate");
+  check(cudaEventCreate(&ev1_), "cudaEventCreate");
+  upload();
+}
+
+Solver::~Solver() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Solver::upload() {
+  const int n = L_.n;
+  const int64_t np = L_.np;
+  int64_t tot = 0;
+  for (int b = 0; b < 2; b++) {
+    f_[b].alloc((size_t)Q * np * sizeof(double));
+    tot += (int64_t)f_[b].bytes;
+    check(cudaMemset(f_[b].p, 0, f_[b].bytes), "cudaMemset");
+  }
+  upload_vec(meta_, L_.meta, tot);
+  upload_vec(run_off_, L_.run_off, tot);
+  upload_vec(st2ref_, L_.st2ref, tot);
+  upload_vec(g_site_, L_.g_site, tot);
+  upload_vec(g_wall_, L_.g_wall, tot);
+  upload_vec(g_iolet_, L_.g_iolet, tot);
+  upload_vec(g_src_, L_.g_src, tot);
+  upload_vec(g_q_, L_.g_q, tot);
+  upload_vec(g_nrm_, L_.g_nrm, tot);
+  upload_vec(g_io_, L_.g_io, tot);
+  upload_vec(g_cpl_, L_.g_cpl, tot);
+  upload_vec(g_xyz_, L_.g_xyz, tot);
+
+  // LES sponge relaxation time per site (LBGKLESSpongeLayer::InitState,
+  // src/lb/kernels/LBGKLESSpongeLayer.h:87-116), in storage order.
+  if (opt_.kernel == kLES) {
+    std::vector<double> vt(n);
+    const double width = p_.sponge_width, widthsq = width * width;
+    for (int s = 0; s < n; s++) {
+      const int x = L_.st2ref[s];
+      double vr = 1.0;
+      for (int k = 0; k < p_.n_outlets; k++) {
+        const double dx = (double)t_.coords[3 * x] - p_.outlets[k].position[0];
+        const double dy = (double)t_.coords[3 * x + 1] - p_.outlets[k].position[1];
+        const double dz = (double)t_.coords[3 * x + 2] - p_.outlets[k].position[2];
+        const double distsq = dx * dx + dy * dy + dz * dz;
+        const double dist = std::sqrt(distsq);
+        if (distsq <= widthsq) vr *= 1.0 + (p_.viscosity_ratio - 1.0) * (dist / width - 1.0) * (dist / width - 1.0);
+      }
+      vt[s] = vr * (p_.tau - 0.5) + 0.5;
+    }
+    upload_vec(vtau_, vt, tot);
+  }
+
+  // Iolet table.
+  std::vector<IoletDev> io(32);
+  std::memset(io.data(), 0, io.size() * sizeof(IoletDev));
+  for (int idx = 0; idx < 32; idx++) {
+    const int cnt = idx < 16 ? p_.n_inlets : p_.n_outlets;
+    if (idx % 16 >= cnt) continue;
+    const hb_iolet& c = idx < 16 ? p_.inlets[idx] : p_.outlets[idx - 16];
+    IoletDev& d = io[idx];
+    d.kind = c.kind;
+    d.dir0 = L_.dir0[idx];
+    d.wk3 = -1;
+    for (int k = 0; k < 3; k++) {
+      d.pos[k] = c.position[k];
+      d.nrm[k] = c.normal[k];
+      d.nrm_f[k] = (double)(float)c.normal[k];
+    }
+    d.radius = c.radius;
+    d.max_speed = c.max_speed;
+    d.warmup = c.warmup;
+  }
+  std::vector<WK3Dev> wk(L_.couplings.size());
+  for (size_t k = 0; k < L_.couplings.size(); k++) {
+    const auto& c = L_.couplings[k];
+    const hb_iolet& cfg = c.iolet < 16 ? p_.inlets[c.iolet] : p_.outlets[c.iolet - 16];
+    WK3Dev& w = wk[k];
+    std::memset(&w, 0, sizeof(w));
+    w.density = w.density_new = 1.0;
+    w.flow = w.flow_old = 0.0;
+    w.rc = cfg.rc;
+    w.rp = cfg.rp;
+    w.cp = cfg.cp;
+    w.area = cfg.area;
+    w.cpl_start = c.start;
+    w.cpl_count = c.count;
+    w.count_prev = 0;
+    w.centre_couples = c.centre_couples ? 1 : 0;
+    w.iolet = c.iolet;
+    io[c.iolet].wk3 = (int)k;
+  }
+  nwk3_ = (int)wk.size();
+  upload_vec(iolets_, io, tot);
+  upload_vec(wk3_, wk, tot);
+  std::vector<double> zeros(std::max(1, L_.cpl_total), 0.0);
+  upload_vec(cpl_buf_, zeros, tot);
+  dens_rows_ = 1024;
+  dens_.alloc((size_t)dens_rows_ * 32 * sizeof(double));
+  tot += (int64_t)dens_.bytes;
+  host_rows_.assign((size_t)dens_rows_ * 32, 1.0);
+  status_.alloc(sizeof(int));
+  check(cudaMemset(status_.p, 0, sizeof(int)), "cudaMemset");
+  dev_bytes_ = tot;
+
+  // Equilibrium initial condition in direct form.
+  double feq[Q];
+  feq_host(p_.initial_density, 0.0, 0.0, 0.0, feq);
+  launch_equilibrium_f64(f_[0].as<double>(), np, n, feq, stream_);
+  check(cudaGetLastError(), "equilibrium fill");
+  cur_ = 0;
+  direct_ = true;
+  check(cudaStreamSynchronize(stream_), "initialisation");
+}
+
+void Solver::ensure_macro() {
+  if (rho_.p) return;
+  rho_.alloc((size_t)L_.np * sizeof(double));
+  u_.alloc((size_t)3 * L_.np * sizeof(double));
+  wss_.alloc((size_t)L_.np * sizeof(double));
+  dev_bytes_ += (int64_t)(rho_.bytes + u_.bytes + wss_.bytes);
+}
+
+StepArgs Solver::args() const {
+  StepArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.fin = f_[cur_].as<double>();
+  a.fout = f_[1 - cur_].as<double>();
+  a.np = L_.np;
+  a.n = L_.n;
+  a.meta = meta_.as<int>();
+  a.run_off = run_off_.as<int>();
+  a.gen.G = L_.G;
+  a.gen.site = g_site_.as<int>();
+  a.gen.wall = g_wall_.as<uint32_t>();
+  a.gen.iolet = g_iolet_.as<uint32_t>();
+  a.gen.src = g_src_.as<int>();
+  a.gen.q = g_q_.as<float>();
+  a.gen.nrm = g_nrm_.as<float>();
+  a.gen.io = g_io_.as<int>();
+  a.gen.cpl = g_cpl_.as<int>();
+  a.gen.xyz = g_xyz_.as<int>();
+  a.tau = p_.tau;
+  a.omega = omega_;
+  a.omega_minus = omega_minus_;
+  a.vtau = vtau_.as<double>();
+  a.t = t_step_;
+  a.lifetime = p_.sponge_lifetime;
+  a.iolets = iolets_.as<IoletDev>();
+  a.dens_row = dens_.as<double>() + (size_t)row_ * 32;
+  a.cpl_buf = cpl_buf_.as<double>();
+  a.rho = rho_.as<double>();
+  a.u = u_.as<double>();
+  a.wss = wss_.as<double>();
+  a.status = status_.as<int>();
+  return a;
+}
+
+// Host-side iolet densities for `count` steps from t_first (1-based): the cosine
+// iolets' GetDensity(t - 1).  Windkessel entries are written on the device.
+void Solver::fill_density_rows(uint64_t t_first, int count) {
+  double mind = 1.7976931348623157e308;
+  for (int k = 0; k < p_.n_inlets + p_.n_outlets; k++) {
+    const hb_iolet& c = k < p_.n_inlets ? p_.inlets[k] : p_.outlets[k - p_.n_inlets];
+    const double dmin = c.kind == kCosine ? c.density_mean - c.density_amp : 1.0;
+    if (dmin < mind) mind = dmin;
+  }
+  for (int r = 0; r < count; r++) {
+    const uint64_t t0 = t_first + (uint64_t)r - 1;
+    for (int idx = 0; idx < 32; idx++) {
+      const int cnt = idx < 16 ? p_.n_inlets : p_.n_outlets;
+      double v = 1.0;
+      if (idx % 16 < cnt) {
+        const hb_iolet& c = idx < 16 ? p_.inlets[idx] : p_.outlets[idx - 16];
+        if (c.kind == kCosine) {
+          const double w = 2.0 * kPi / c.period;
+          const double target = c.density_mean + c.density_amp * std::cos(w * (double)t0 + c.phase);
+          if (t0 >= c.warmup) v = target;
+          else {
+            const double fac = ((double)t0) / ((double)c.warmup);
+            v = fac * target + (1. - fac) * mind;
+          }
+        }
+      }
+      host_rows_[(size_t)r * 32 + idx] = v;
+    }
+  }
+  check(cudaMemcpyAsync(dens_.p, host_rows_.data(), (size_t)count * 32 * sizeof(double), cudaMemcpyHostToDevice, stream_),
+        "density table upload");
+}
+
+void Solver::request_comms() {
+  if (!phase_open_) {
+    fill_density_rows(t_step_, 1);
+    row_ = 0;
+  }
+  launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * 32, stream_);
+  phase_open_ = true;
+}
+
+void Solver::pre_receive(bool macro, int which) {
+  if (!phase_open_) request_comms();
+  if (macro) ensure_macro();
+  launch_step_f64(args(), opt_.kernel, opt_.wall, !direct_, macro, which, 256, 128, stream_);
+  check(cudaGetLastError(), "step kernel launch");
+  phase_macro_ = macro;
+}
+
+void Solver::end_iteration() {
+  prev_direct_ = direct_;
+  prev_valid_ = true;
+  cur_ = 1 - cur_;
+  direct_ = false;
+  t_step_++;
+  phase_open_ = false;
+  macro_valid_ = phase_macro_;
+  phase_macro_ = false;
+}
+
+int Solver::read_status() {
+  int st = 0;
+  check(cudaMemcpyAsync(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "status read");
+  check(cudaStreamSynchronize(stream_), "step");
+  if (st) {
+    status_sticky_ |= st;
+    check(cudaMemsetAsync(status_.p, 0, sizeof(int), stream_), "status reset");
+  }
+  return st;
+}
+
+int Solver::step(int64_t nsteps, uint32_t flags) {
+  if (nsteps < 0) throw Error{HB_ERR_ARG, "negative step count"};
+  int64_t launches = 0;
+  const int per_step = (nwk3_ ? 1 : 0) + (L_.n > 0 ? 1 : 0) + (L_.G > 0 ? 1 : 0);
+  check(cudaEventRecord(ev0_, stream_), "event");
+  int64_t done = 0;
+  while (done < nsteps) {
+    const int chunk = (int)std::min<int64_t>(dens_rows_, nsteps - done);
+    fill_density_rows(t_step_, chunk);
+    for (int j = 0; j < chunk; j++) {
+      row_ = j;
+      phase_open_ = true;
+      launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * 32, stream_);
+      const bool macro = (flags & HB_STEP_MACRO) && (done + j == nsteps - 1);
+      pre_receive(macro);
+      end_iteration();
+      launches += per_step;
+    }
+    done += chunk;
+  }
+  check(cudaEventRecord(ev1_, stream_), "event");
+  const int st = read_status();
+  float ms = 0;
+  check(cudaEventElapsedTime(&ms, ev0_, ev1_), "event timing");
+  last_ms_ = ms;
+  last_launches_ = launches;
+  if (st & kStatusIoletRadius) return HB_ERR_IOLET_RADIUS;
+  if (st & kStatusUnstable) return HB_UNSTABLE;
+  return HB_OK;
+}
+
+int Solver::profile(int64_t nsteps, double ms[3]) {
+  ms[0] = ms[1] = ms[2] = 0.0;
+  cudaEvent_t e[4];
+  for (auto& x : e) check(cudaEventCreate(&x), "cudaEventCreate");
+  int64_t done = 0;
+  int rc = HB_OK;
+  while (done < nsteps) {
+    const int chunk = (int)std::min<int64_t>(dens_rows_, nsteps - done);
+    fill_density_rows(t_step_, chunk);
+    for (int j = 0; j < chunk; j++) {
+      row_ = j;
+      phase_open_ = true;
+      check(cudaEventRecord(e[0], stream_), "event");
+      launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * 32, stream_);
+      check(cudaEventRecord(e[1], stream_), "event");
+      pre_receive(false, 1);
+      check(cudaEventRecord(e[2], stream_), "event");
+      pre_receive(false, 2);
+      check(cudaEventRecord(e[3], stream_), "event");
+      end_iteration();
+      check(cudaEventSynchronize(e[3]), "event sync");
+      float a = 0, b = 0, c = 0;
+      check(cudaEventElapsedTime(&a, e[0], e[1]), "event");
+      check(cudaEventElapsedTime(&b, e[1], e[2]), "event");
+      check(cudaEventElapsedTime(&c, e[2], e[3]), "event");
+      ms[2] += a;
+      ms[0] += b;
+      ms[1] += c;
+    }
+    done += chunk;
+  }
+  for (auto& x : e) cudaEventDestroy(x);
+  const int st = read_status();
+  if (st & kStatusIoletRadius) rc = HB_ERR_IOLET_RADIUS;
+  else if (st & kStatusUnstable) rc = HB_UNSTABLE;
+  return rc;
+}
+
+// Turn post-collision f* into the pre-collision f the reference holds in f_old.
+void Solver::materialise() {
+  if (direct_) return;
+  StepArgs a = args();
+  launch_gather_f64(a, opt_.wall, stream_);
+  check(cudaGetLastError(), "gather launch");
+  cur_ = 1 - cur_;
+  direct_ = true;
+  prev_valid_ = false;
+}
+
+bool Solver::get_previous_fs(double* f) {
+  if (!prev_valid_) return false;
+  DeviceBuffer tmp;
+  tmp.alloc((size_t)L_.n * Q * sizeof(double));
+  StepArgs a = args();
+  a.fin = f_[1 - cur_].as<double>();
+  if (prev_direct_) {
+    launch_soa_to_aos_f64(a.fin, L_.np, st2ref_.as<int>(), L_.n, tmp.as<double>(), stream_);
+  } else {
+    launch_gather_aos_f64(a, opt_.wall, st2ref_.as<int>(), tmp.as<double>(), stream_);
+  }
+  check(cudaGetLastError(), "previous-state gather");
+  check(cudaMemcpyAsync(f, tmp.p, (size_t)L_.n * Q * sizeof(double), cudaMemcpyDeviceToHost, stream_), "f download");
+  check(cudaStreamSynchronize(stream_), "get_previous_fs");
+  return true;
+}
+
+void Solver::set_units(double dt, double dx, const double origin[3]) {
+  dt_ = dt;
+  dx_ = dx;
+  for (int k = 0; k < 3; k++) origin_[k] = origin[k];
+}
+
+void Solver::get_fs(double* f) {
+  materialise();
+  double* aos = f_[1 - cur_].as<double>();  // the spare buffer holds n*19 doubles
+  launch_soa_to_aos_f64(f_[cur_].as<double>(), L_.np, st2ref_.as<int>(), L_.n, aos, stream_);
+  check(cudaGetLastError(), "soa_to_aos launch");
+  check(cudaMemcpyAsync(f, aos, (size_t)L_.n * Q * sizeof(double), cudaMemcpyDeviceToHost, stream_), "f download");
+  check(cudaStreamSynchronize(stream_), "get_fs");
+}
+
+void Solver::set_fs(const double* f) {
+  double* aos = f_[1 - cur_].as<double>();
+  check(cudaMemcpyAsync(aos, f, (size_t)L_.n * Q * sizeof(double), cudaMemcpyHostToDevice, stream_), "f upload");
+  launch_aos_to_soa_f64(aos, st2ref_.as<int>(), L_.n, f_[cur_].as<double>(), L_.np, stream_);
+  check(cudaGetLastError(), "aos_to_soa launch");
+  direct_ = true;
+  prev_valid_ = false;
+  check(cudaStreamSynchronize(stream_), "set_fs");
+}
+
+void Solver::get_macro(double* rho, double* u, double* wss) {
+  if (!macro_valid_ || !rho_.p) throw Error{HB_ERR_ARG, "no step has filled the macroscopic caches (pass HB_STEP_MACRO)"};
+  const int n = L_.n;
+  const int64_t np = L_.np;
+  std::vector<double> r(np), uu(3 * np), w(np);
+  check(cudaMemcpyAsync(r.data(), rho_.p, np * sizeof(double), cudaMemcpyDeviceToHost, stream_), "macro download");
+  check(cudaMemcpyAsync(uu.data(), u_.p, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, stream_), "macro download");
+  check(cudaMemcpyAsync(w.data(), wss_.p, np * sizeof(double), cudaMemcpyDeviceToHost, stream_), "macro download");
+  check(cudaStreamSynchronize(stream_), "get_macro");
+  for (int s = 0; s < n; s++) {
+    const int x = L_.st2ref[s];
+    if (rho) rho[x] = r[s];
+    if (u) {
+      u[3 * x] = uu[s];
+      u[3 * x + 1] = uu[np + s];
+      u[3 * x + 2] = uu[2 * np + s];
+    }
+    if (wss) wss[x] = w[s];
+  }
+}
+
+void Solver::get_wk3(int group, int index, double st[4]) {
+  const int idx = group * 16 + index;
+  for (size_t k = 0; k < L_.couplings.size(); k++) {
+    if (L_.couplings[k].iolet != idx) continue;
+    WK3Dev w;
+    check(cudaMemcpyAsync(&w, wk3_.as<WK3Dev>() + k, sizeof(WK3Dev), cudaMemcpyDeviceToHost, stream_), "wk3 download");
+    check(cudaStreamSynchronize(stream_), "get_wk3");
+    st[0] = w.density;
+    st[1] = w.density_new;
+    st[2] = w.flow;
+    st[3] = w.flow_old;
+    return;
+  }
+  throw Error{HB_ERR_ARG, "iolet is not a Windkessel iolet"};
+}
+
+}  // namespace hb

@@ -1,0 +1,110 @@
+// solver.h -- one lattice resident on one GPU (the state behind an hb_handle).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/hemeb200.h"
+#include "config.h"
+#include "device.h"
+#include "layout.h"
+
+namespace hb {
+
+struct DeviceBuffer {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer();
+  void alloc(size_t b);
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+class Solver {
+ public:
+  Solver(LatticeTables tables, const hb_params& params, const hb_options& opt);
+  ~Solver();
+
+  // lb::LBM phases.
+  void request_comms();
+  void pre_receive(bool macro, int which = 3);
+  void end_iteration();
+  int step(int64_t n, uint32_t flags);
+  // `n` steps with CUDA events around each launch: ms[0] plain bulk kernel,
+  // ms[1] general kernel, ms[2] Windkessel kernel (summed over the steps).
+  int profile(int64_t n, double ms[3]);
+
+  void get_fs(double* f);
+  void set_fs(const double* f);
+  void get_macro(double* rho, double* u, double* wss);
+  void get_wk3(int group, int index, double st[4]);
+
+  const LatticeTables& tables() const { return t_; }
+  const Layout& layout() const { return L_; }
+  const hb_params& params() const { return p_; }
+  uint64_t time_step() const { return t_step_; }
+  double last_ms() const { return last_ms_; }
+  int64_t last_launches() const { return last_launches_; }
+  int64_t device_bytes() const { return dev_bytes_; }
+  int read_status();
+
+  // Physical scales for output (UnitConverter): time step, voxel size, origin.
+  void set_units(double dt, double dx, const double origin[3]);
+  double dt() const { return dt_; }
+  double dx() const { return dx_; }
+  const double* origin() const { return origin_; }
+  bool macro_valid() const { return macro_valid_; }
+  // Pre-collision f of the last completed step (what the reference's GetFNew
+  // returns after EndIteration), AoS in reference order.  False if no step has
+  // run since the last set_fs / get_fs.
+  bool get_previous_fs(double* f);
+  void set_time_step(uint64_t t) { t_step_ = t; }
+
+ private:
+  void upload();
+  void materialise();
+  void ensure_macro();
+  void fill_density_rows(uint64_t t_first, int count);
+  StepArgs args() const;
+  void check(cudaError_t e, const char* what);
+
+  LatticeTables t_;
+  hb_params p_;
+  hb_options opt_;
+  Layout L_;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+
+  DeviceBuffer f_[2];
+  int cur_ = 0;
+  bool direct_ = true;            // f_[cur_] holds pre-collision f (else post-collision f*)
+  DeviceBuffer meta_, run_off_, st2ref_;
+  DeviceBuffer g_site_, g_wall_, g_iolet_, g_src_, g_q_, g_nrm_, g_io_, g_cpl_, g_xyz_;
+  DeviceBuffer vtau_, iolets_, dens_, cpl_buf_, wk3_, status_;
+  DeviceBuffer rho_, u_, wss_;
+  int dens_rows_ = 0;
+  int row_ = 0;                   // row of the density table used by the current step
+  std::vector<double> host_rows_;
+  int nwk3_ = 0;
+  bool macro_valid_ = false;
+  bool phase_open_ = false;
+  bool phase_macro_ = false;
+  uint64_t t_step_ = 1;
+  double omega_ = 0, omega_minus_ = 0;
+  double last_ms_ = 0;
+  int64_t last_launches_ = 0;
+  int64_t dev_bytes_ = 0;
+  int status_sticky_ = 0;
+  bool prev_valid_ = false;
+  bool prev_direct_ = false;
+  double dt_ = 1.0, dx_ = 1.0;
+  double origin_[3] = {0, 0, 0};
+};
+
+}  // namespace hb

@@ -1,0 +1,358 @@
+"""Python mirror of the reference's lb::LBM interface over the C ABI (libhemeb200.so).
+
+The reference drives one time step as RequestComms, PreSend, PreReceive,
+PostReceive, EndIteration (src/lb/lb.hpp:191-346); this class keeps those names
+and argument meanings.  Distributions and site arrays are in the reference's
+contiguous site order.  Errors raise `HemeLBError` carrying the HB_* status,
+as the reference throws hemelb::Exception; instability is reported as
+`Unstable` (the reference's SimulationState::SetStability(Unstable)).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhemeb200.so")
+
+HB_OK = 0
+HB_UNSTABLE = 1
+STATUS_NAMES = {1: "HB_UNSTABLE", -1: "HB_ERR_ARG", -2: "HB_ERR_IO", -3: "HB_ERR_FORMAT", -4: "HB_ERR_CUDA",
+                -5: "HB_ERR_OOM", -6: "HB_ERR_BAD_INDEX", -7: "HB_ERR_UNSUPPORTED", -8: "HB_ERR_IOLET_RADIUS",
+                -9: "HB_ERR_TIMEOUT"}
+KERNELS = {"LBGK": 0, "TRT": 1, "LBGKLESSL": 2}
+WALLS = {"SBB": 0, "BFL": 1, "GZS": 2}
+PRECISIONS = {"fp64": 0, "fp32": 1, "fp16": 2}
+IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2}
+STEP_MACRO = 1
+
+# Every entry point include/hemeb200.h declares.
+EXPORTS = [
+    "hb_default_options", "hb_create_from_xml", "hb_create", "hb_destroy", "hb_last_error",
+    "hb_request_comms", "hb_pre_send", "hb_pre_receive", "hb_post_receive", "hb_end_iteration",
+    "hb_step", "hb_site_count", "hb_time_step", "hb_get_params", "hb_get_fs", "hb_set_fs",
+    "hb_get_macro", "hb_get_wk3", "hb_get_tables", "hb_write_xtr", "hb_read_checkpoint",
+    "hb_last_step_timing", "hb_device_bytes", "hb_read_case", "hb_geometry_open", "hb_geometry_site_count",
+    "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_close", "hb_profile_steps",
+]
+
+
+class HemeLBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Unstable(HemeLBError):
+    pass
+
+
+class Options(C.Structure):
+    _fields_ = [("kernel", C.c_int), ("wall", C.c_int), ("precision", C.c_int), ("device", C.c_int)]
+
+
+class Iolet(C.Structure):
+    _fields_ = [("kind", C.c_int), ("position", C.c_double * 3), ("normal", C.c_double * 3),
+                ("density_mean", C.c_double), ("density_amp", C.c_double), ("phase", C.c_double),
+                ("period", C.c_double), ("warmup", C.c_uint64), ("radius", C.c_double),
+                ("max_speed", C.c_double), ("rc", C.c_double), ("rp", C.c_double), ("cp", C.c_double),
+                ("area", C.c_double)]
+
+
+class Params(C.Structure):
+    _fields_ = [("tau", C.c_double), ("relaxation_parameter", C.c_double), ("viscosity_ratio", C.c_double),
+                ("sponge_width", C.c_double), ("sponge_lifetime", C.c_uint64), ("initial_density", C.c_double),
+                ("initial_step", C.c_uint64), ("n_inlets", C.c_int), ("n_outlets", C.c_int),
+                ("inlets", Iolet * 16), ("outlets", Iolet * 16)]
+
+
+class LatticeDesc(C.Structure):
+    _fields_ = [("n_sites", C.c_int64), ("dims", C.c_int64 * 3), ("coords", C.c_void_p),
+                ("wall_mask", C.c_void_p), ("iolet_mask", C.c_void_p), ("site_type", C.c_void_p),
+                ("iolet_id", C.c_void_p), ("wall_distance", C.c_void_p), ("wall_normal", C.c_void_p),
+                ("neighbours", C.c_void_p)]
+
+
+_lib = None
+
+
+def library() -> C.CDLL:
+    """Load libhemeb200.so; raise if it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m hemepure_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P, I, I64, U32, U64 = C.c_void_p, C.c_int, C.c_int64, C.c_uint32, C.c_uint64
+    L.hb_default_options.argtypes = [P]
+    L.hb_default_options.restype = None
+    L.hb_create_from_xml.argtypes = [C.c_char_p, P, C.POINTER(P)]
+    L.hb_create.argtypes = [P, P, P, C.POINTER(P)]
+    L.hb_destroy.argtypes = [P]
+    L.hb_last_error.argtypes = [P, C.c_char_p, C.c_size_t]
+    for name in ("hb_request_comms", "hb_pre_send", "hb_post_receive", "hb_end_iteration"):
+        getattr(L, name).argtypes = [P]
+    L.hb_pre_receive.argtypes = [P, U32]
+    L.hb_step.argtypes = [P, I64, U32]
+    L.hb_site_count.argtypes = [P, P]
+    L.hb_time_step.argtypes = [P, P]
+    L.hb_get_params.argtypes = [P, P]
+    L.hb_get_fs.argtypes = [P, P]
+    L.hb_set_fs.argtypes = [P, P]
+    L.hb_get_macro.argtypes = [P, P, P, P]
+    L.hb_get_wk3.argtypes = [P, I, I, P]
+    L.hb_get_tables.argtypes = [P, P, P, P, P, P, P, P]
+    L.hb_write_xtr.argtypes = [P, C.c_char_p, C.c_char_p, C.c_char_p]
+    L.hb_read_checkpoint.argtypes = [P, C.c_char_p, U64]
+    L.hb_last_step_timing.argtypes = [P, P, P]
+    L.hb_device_bytes.argtypes = [P, P]
+    L.hb_read_case.argtypes = [C.c_char_p, I, P, C.c_char_p, C.c_size_t]
+    L.hb_geometry_open.argtypes = [C.c_char_p, C.POINTER(P)]
+    L.hb_geometry_site_count.argtypes = [P, P, P]
+    L.hb_geometry_tables.argtypes = [P] + [P] * 9
+    L.hb_geometry_layout.argtypes = [P, P, I, P]
+    L.hb_geometry_close.argtypes = [P]
+    L.hb_profile_steps.argtypes = [P, I64, P]
+    for name in EXPORTS:
+        fn = getattr(L, name)
+        if name != "hb_default_options":
+            fn.restype = I
+    _lib = L
+    return L
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def options(kernel="LBGK", wall="SBB", precision="fp64", device=0) -> Options:
+    o = Options()
+    library().hb_default_options(C.byref(o))
+    o.kernel = KERNELS[kernel]
+    o.wall = WALLS[wall]
+    o.precision = PRECISIONS[precision]
+    o.device = int(device)
+    return o
+
+
+class LBM:
+    """One lattice resident on one GPU: the reference's lb::LBM<D3Q19>."""
+
+    def __init__(self, xml_path: Optional[str] = None, kernel: str = "LBGK", wall: str = "SBB",
+                 precision: str = "fp64", device: int = 0, lattice: Optional[Dict[str, np.ndarray]] = None,
+                 params: Optional[Params] = None):
+        L = library()
+        self._h = C.c_void_p()
+        self._opt = options(kernel, wall, precision, device)
+        if xml_path is not None:
+            rc = L.hb_create_from_xml(os.fspath(xml_path).encode(), C.byref(self._opt), C.byref(self._h))
+        else:
+            if lattice is None or params is None:
+                raise ValueError("pass an XML case file, or lattice tables and parameters")
+            self._keep = {k: np.ascontiguousarray(v) for k, v in lattice.items() if v is not None}
+            d = LatticeDesc()
+            d.n_sites = int(self._keep["coords"].shape[0])
+            d.dims[:] = [int(v) for v in lattice["dims"]]
+            for name, key, dt in (("coords", "coords", np.int64), ("wall_mask", "wall_mask", np.uint32),
+                                  ("iolet_mask", "iolet_mask", np.uint32), ("site_type", "site_type", np.int32),
+                                  ("iolet_id", "iolet_id", np.int32), ("wall_distance", "wall_distance", np.float64),
+                                  ("wall_normal", "wall_normal", np.float64), ("neighbours", "neighbours", np.int64)):
+                if key in self._keep:
+                    self._keep[key] = np.ascontiguousarray(self._keep[key], dtype=dt)
+                    setattr(d, name, _p(self._keep[key]))
+            rc = L.hb_create(C.byref(d), C.byref(params), C.byref(self._opt), C.byref(self._h))
+        if rc != HB_OK:
+            raise HemeLBError(rc, self._error(None))
+        n = C.c_int64()
+        L.hb_site_count(self._h, C.byref(n))
+        self.n = int(n.value)
+
+    # -- housekeeping -----------------------------------------------------------
+    def _error(self, h) -> str:
+        buf = C.create_string_buffer(1024)
+        library().hb_last_error(h, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc: int) -> int:
+        if rc == HB_OK:
+            return rc
+        if rc == HB_UNSTABLE:
+            raise Unstable(rc, "the simulation became unstable (some f <= 0 or NaN)")
+        raise HemeLBError(rc, self._error(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            library().hb_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- lb::LBM per-step phases -------------------------------------------------------
+    def RequestComms(self) -> None:
+        self._check(library().hb_request_comms(self._h))
+
+    def PreSend(self) -> None:
+        self._check(library().hb_pre_send(self._h))
+
+    def PreReceive(self, macro: bool = False) -> None:
+        self._check(library().hb_pre_receive(self._h, STEP_MACRO if macro else 0))
+
+    def PostReceive(self) -> None:
+        self._check(library().hb_post_receive(self._h))
+
+    def EndIteration(self) -> None:
+        self._check(library().hb_end_iteration(self._h))
+
+    def step(self, n: int = 1, macro: bool = False) -> None:
+        """`n` full time steps (all phases); `macro` fills the caches on the last."""
+        self._check(library().hb_step(self._h, int(n), STEP_MACRO if macro else 0))
+
+    # -- state ---------------------------------------------------------------------------
+    @property
+    def time_step(self) -> int:
+        t = C.c_uint64()
+        library().hb_time_step(self._h, C.byref(t))
+        return int(t.value)
+
+    def GetLbmParams(self) -> Params:
+        p = Params()
+        self._check(library().hb_get_params(self._h, C.byref(p)))
+        return p
+
+    def GetFOld(self) -> np.ndarray:
+        """Distributions entering the next step, [n, 19] in reference order."""
+        f = np.empty((self.n, 19), np.float64)
+        self._check(library().hb_get_fs(self._h, _p(f)))
+        return f
+
+    def SetFs(self, f: np.ndarray) -> None:
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        if f.shape != (self.n, 19):
+            raise ValueError(f"expected shape {(self.n, 19)}")
+        self._check(library().hb_set_fs(self._h, _p(f)))
+
+    def GetPropertyCache(self):
+        """(density [n], velocity [n, 3], wall-shear-stress [n]) of the last macro step."""
+        rho = np.empty(self.n)
+        u = np.empty((self.n, 3))
+        w = np.empty(self.n)
+        self._check(library().hb_get_macro(self._h, _p(rho), _p(u), _p(w)))
+        return rho, u, w
+
+    def GetWK3(self, group: int, index: int) -> np.ndarray:
+        a = np.empty(4)
+        self._check(library().hb_get_wk3(self._h, int(group), int(index), _p(a)))
+        return a
+
+    def tables(self) -> Dict[str, np.ndarray]:
+        n = self.n
+        out = {"neighbours": np.empty((n, 19), np.int64), "wall_mask": np.empty(n, np.uint32),
+               "iolet_mask": np.empty(n, np.uint32), "site_type": np.empty(n, np.int32),
+               "iolet_id": np.empty(n, np.int32), "coords": np.empty((n, 3), np.int64),
+               "type_counts": np.empty(6, np.int64)}
+        self._check(library().hb_get_tables(self._h, *(_p(out[k]) for k in (
+            "neighbours", "wall_mask", "iolet_mask", "site_type", "iolet_id", "coords", "type_counts"))))
+        return out
+
+    def WriteXtr(self, path: str, fields: Sequence[str], offset_path: Optional[str] = None) -> None:
+        self._check(library().hb_write_xtr(self._h, os.fspath(path).encode(), ",".join(fields).encode(),
+                                           os.fspath(offset_path).encode() if offset_path else None))
+
+    def ReadCheckpoint(self, path: str, step: int = 0) -> None:
+        self._check(library().hb_read_checkpoint(self._h, os.fspath(path).encode(), int(step)))
+
+    def last_step_timing(self):
+        ms = C.c_double()
+        n = C.c_int64()
+        library().hb_last_step_timing(self._h, C.byref(ms), C.byref(n))
+        return float(ms.value), int(n.value)
+
+    def profile_steps(self, n: int):
+        """Advance `n` steps timing each launch: (bulk ms, general ms, windkessel ms)."""
+        ms = np.zeros(3)
+        self._check(library().hb_profile_steps(self._h, int(n), _p(ms)))
+        return float(ms[0]), float(ms[1]), float(ms[2])
+
+    def device_bytes(self) -> int:
+        b = C.c_int64()
+        library().hb_device_bytes(self._h, C.byref(b))
+        return int(b.value)
+
+
+def last_create_error() -> str:
+    buf = C.create_string_buffer(1024)
+    library().hb_last_error(None, buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def read_case(xml_path: str, kernel: str = "LBGK"):
+    """(Params, gmy path) as the library's case reader sees them (no GPU needed)."""
+    p = Params()
+    buf = C.create_string_buffer(4096)
+    rc = library().hb_read_case(os.fspath(xml_path).encode(), KERNELS[kernel], C.byref(p), buf, 4096)
+    if rc != HB_OK:
+        raise HemeLBError(rc, last_create_error())
+    return p, buf.value.decode()
+
+
+class Geometry:
+    """Reference-order lattice tables read by the library's host code (no GPU needed)."""
+
+    def __init__(self, gmy_path: str):
+        self._g = C.c_void_p()
+        rc = library().hb_geometry_open(os.fspath(gmy_path).encode(), C.byref(self._g))
+        if rc != HB_OK:
+            raise HemeLBError(rc, last_create_error())
+        n = C.c_int64()
+        dims = np.zeros(3, np.int64)
+        library().hb_geometry_site_count(self._g, C.byref(n), _p(dims))
+        self.n = int(n.value)
+        self.dims = dims
+
+    def tables(self) -> Dict[str, np.ndarray]:
+        n = self.n
+        out = {"neighbours": np.empty((n, 19), np.int64), "wall_mask": np.empty(n, np.uint32),
+               "iolet_mask": np.empty(n, np.uint32), "site_type": np.empty(n, np.int32),
+               "iolet_id": np.empty(n, np.int32), "coords": np.empty((n, 3), np.int64),
+               "type_counts": np.empty(6, np.int64), "wall_distance": np.empty((n, 18)),
+               "wall_normal": np.empty((n, 3))}
+        rc = library().hb_geometry_tables(self._g, *(_p(out[k]) for k in (
+            "neighbours", "wall_mask", "iolet_mask", "site_type", "iolet_id", "coords", "type_counts",
+            "wall_distance", "wall_normal")))
+        if rc != HB_OK:
+            raise HemeLBError(rc, last_create_error())
+        out["dims"] = self.dims.copy()
+        return out
+
+    def layout(self, params: Params, wall: str = "SBB") -> Dict[str, int]:
+        st = np.zeros(4, np.int64)
+        rc = library().hb_geometry_layout(self._g, C.byref(params), WALLS[wall], _p(st))
+        if rc != HB_OK:
+            raise HemeLBError(rc, last_create_error())
+        return {"axis": int(st[0]), "runs": int(st[1]), "bulk_sites": int(st[2]), "general_sites": int(st[3])}
+
+    def close(self):
+        if getattr(self, "_g", None) and self._g.value:
+            library().hb_geometry_close(self._g)
+            self._g = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

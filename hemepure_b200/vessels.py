@@ -559,6 +559,13 @@ def make_case(name: str, out_dir: str, steps: Optional[int] = None, scale: float
         u = CaseUnits(tau=0.55)
         write_case_xml(xml, os.path.basename(gmy), v, u, steps or 4000,
                        [VelocityBC(0.02)], [PressureBC(1.0)], warmup=1000)
+    elif name == "pipe_r40_short":
+        # The large pipe's cross-section and physics over 200 slices (1,004,800
+        # sites): the case the kernel profiles capture.
+        v = Pipe(sc(40), sc(200, 8))
+        u = CaseUnits(tau=0.55)
+        write_case_xml(xml, os.path.basename(gmy), v, u, steps or 4000,
+                       [VelocityBC(0.02)], [PressureBC(1.0)], warmup=1000)
     elif name == "bifurcation":
         # Y-bifurcation, TRT (magic 3/16, tau+=0.52), GZS walls, cosine pressure
         # inlet (mean 1, amplitude 1e-3, period 4000), two WK3 outlets.

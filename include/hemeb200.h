@@ -1,0 +1,217 @@
+/*
+ * hemeb200.h -- C ABI of the B200 D3Q19 collide-and-stream library (libhemeb200.so).
+ *
+ * The library replaces the per-time-step work of the reference's lb::LBM
+ * (src/lb/lb.h:32-148, src/lb/lb.hpp:119-346): the six streamers run over the
+ * type-contiguous site ranges in PreSend/PreReceive, the post-step fix-ups in
+ * PostReceive and the swap in EndIteration.  Everything the reference keeps in
+ * geometry::LatticeData for that path (distributions, neighbour indices, site
+ * data, wall distances and normals; src/geometry/LatticeData.h:624-653) lives in
+ * device memory behind an opaque handle.
+ *
+ * All functions return an int status: HB_OK (0) on success, a positive value for
+ * a numerical condition (HB_UNSTABLE), a negative value for an error.  Nothing
+ * throws across the ABI.  Site-indexed host arrays are in the reference's
+ * contiguous site order (collision types 0..5, each in block-traversal order),
+ * and distributions are AoS [site*19 + direction] doubles, exactly as the
+ * reference stores f_old/f_new.  One host thread per handle.
+ */
+#ifndef HEMEB200_H
+#define HEMEB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (reference: hemelb::Exception / SimulationState::SetStability) */
+#define HB_OK 0
+#define HB_UNSTABLE 1            /* some f <= 0 or NaN (src/lb/StabilityTester.h:100-111) */
+#define HB_ERR_ARG (-1)          /* bad argument or handle */
+#define HB_ERR_IO (-2)           /* file cannot be read or written */
+#define HB_ERR_FORMAT (-3)       /* malformed XML / .gmy / .xtr */
+#define HB_ERR_CUDA (-4)         /* a CUDA call failed */
+#define HB_ERR_OOM (-5)          /* device memory exhausted */
+#define HB_ERR_BAD_INDEX (-6)    /* a site or neighbour table failed validation */
+#define HB_ERR_UNSUPPORTED (-7)  /* configuration outside the supported set */
+#define HB_ERR_IOLET_RADIUS (-8) /* parabolic iolet point outside its radius (reference exit(16)) */
+#define HB_ERR_TIMEOUT (-9)      /* a bounded device wait gave up */
+
+/* ---- run-time selectable types (reference: compile-time CMake strings,
+ *      src/CMakeLists.txt:43-65, src/lb/BuildSystemInterface.h:24-369) */
+#define HB_KERNEL_LBGK 0         /* src/lb/kernels/LBGK.h */
+#define HB_KERNEL_TRT 1          /* src/lb/kernels/TRT.h */
+#define HB_KERNEL_LBGKLESSL 2    /* src/lb/kernels/LBGKLESSpongeLayer.h */
+
+#define HB_WALL_SBB 0            /* src/lb/streamers/SimpleBounceBackDelegate.h */
+#define HB_WALL_BFL 1            /* src/lb/streamers/BouzidiFirdaousLallemandDelegate.h */
+#define HB_WALL_GZS 2            /* src/lb/streamers/GuoZhengShiDelegate.h */
+
+#define HB_IOLET_COSINE 0        /* Nash pressure, src/lb/iolets/InOutLetCosine.cc */
+#define HB_IOLET_WK3 1           /* Nash pressure, src/lb/iolets/InOutLetWK3.cc */
+#define HB_IOLET_PARABOLIC 2     /* Ladd velocity, src/lb/iolets/InOutLetParabolicVelocity.cc */
+
+/* ---- storage precision of the distributions */
+#define HB_STORE_FP64 0          /* plain form: FP64 storage and arithmetic */
+#define HB_STORE_FP32 1          /* f - w_i rho0 stored in FP32, FP32 collision */
+#define HB_STORE_FP16 2          /* f - w_i rho0 stored in FP16, FP32 collision */
+
+/* ---- hb_step flags */
+#define HB_STEP_MACRO 1u         /* fill density, velocity and wall-shear-stress on the last step */
+
+typedef struct hb_handle hb_handle;
+
+typedef struct hb_options {
+  int kernel;     /* HB_KERNEL_* (the reference's HEMELB_KERNEL) */
+  int wall;       /* HB_WALL_* (the reference's HEMELB_WALL_BOUNDARY) */
+  int precision;  /* HB_STORE_* */
+  int device;     /* CUDA device ordinal */
+} hb_options;
+
+/* One inlet or outlet in lattice units (reference: iolets::InOutLet and subclasses). */
+typedef struct hb_iolet {
+  int kind;                 /* HB_IOLET_* */
+  double position[3];       /* InOutLet::GetPosition */
+  double normal[3];         /* normalised; points into the fluid (InOutLet::SetNormal) */
+  double density_mean, density_amp, phase, period; /* cosine (InOutLetCosine) */
+  uint64_t warmup;          /* extra_warmup_steps */
+  double radius, max_speed; /* parabolic (InOutLetParabolicVelocity) */
+  double rc, rp, cp, area;  /* WK3 (InOutLetWK3) */
+} hb_iolet;
+
+/* LbmParameters + iolet set + initial condition, all in lattice units. */
+typedef struct hb_params {
+  double tau;                   /* LbmParameters::GetTau (src/lb/LbmParameters.h:29-37) */
+  double relaxation_parameter;  /* TRT magic number (SimConfig relaxation_parameter) */
+  double viscosity_ratio;       /* LES sponge layer */
+  double sponge_width;          /* lattice units */
+  uint64_t sponge_lifetime;
+  double initial_density;       /* equilibrium initial condition (InitialCondition.cc:71-73) */
+  uint64_t initial_step;        /* 1-based SimulationState time step */
+  int n_inlets, n_outlets;
+  hb_iolet inlets[16];
+  hb_iolet outlets[16];
+} hb_params;
+
+/* The lattice as the reference's LatticeData holds it after
+ * LatticeData::ProcessReadSites / InitialiseNeighbourLookup on one rank. */
+typedef struct hb_lattice_desc {
+  int64_t n_sites;
+  int64_t dims[3];              /* global lattice extent in sites */
+  const int64_t* coords;        /* [n*3] GetGlobalSiteCoords */
+  const uint32_t* wall_mask;    /* [n] SiteData::GetWallIntersectionData */
+  const uint32_t* iolet_mask;   /* [n] SiteData::GetIoletIntersectionData */
+  const int32_t* site_type;     /* [n] 0 fluid, 1 inlet, 2 outlet (geometry::SiteType) */
+  const int32_t* iolet_id;      /* [n] SiteData::GetIoletId */
+  const double* wall_distance;  /* [n*18] GetCutDistance(site, 1..18); may be NULL for SBB */
+  const double* wall_normal;    /* [n*3] GetNormalToWall; may be NULL */
+  const int64_t* neighbours;    /* [n*19] neighbourIndices, or NULL to derive from coords */
+} hb_lattice_desc;
+
+/* ---- construction / teardown ------------------------------------------- */
+
+/* Default options: LBGK, SBB, FP64, device 0. */
+void hb_default_options(hb_options* opt);
+
+/* Build from a case file: SimConfig::New (src/configuration/SimConfig.cc:41-121),
+ * GeometryReader::LoadAndDecompose (src/geometry/GeometryReader.cc:63-365),
+ * new LatticeData, LBM ctor + Initialise + SetInitialConditions. */
+int hb_create_from_xml(const char* xml_path, const hb_options* opt, hb_handle** out);
+
+/* Build from lattice tables the caller already holds (the drop-in path: the
+ * reference keeps its GeometryReader/LatticeData and hands the tables over). */
+int hb_create(const hb_lattice_desc* lat, const hb_params* params, const hb_options* opt, hb_handle** out);
+
+int hb_destroy(hb_handle* h);
+
+/* Last error message of this handle (or of the last failed create when h is NULL). */
+int hb_last_error(const hb_handle* h, char* msg, size_t len);
+
+/* ---- lb::LBM per-step phases (src/lb/lb.hpp:191-346) ------------------------ */
+
+/* BeginPhase: LBM::RequestComms + BoundaryValues::RequestComms (no halo on one GPU;
+ * Windkessel state advances on the device). */
+int hb_request_comms(hb_handle* h);
+/* LBM::PreSend: domain-edge sites; none on one GPU, kept for the call sequence. */
+int hb_pre_send(hb_handle* h);
+/* LBM::PreReceive: collide and stream every site (all six collision types). */
+int hb_pre_receive(hb_handle* h, uint32_t flags);
+/* LBM::PostReceive: the post-step fix-ups are folded into the next gather. */
+int hb_post_receive(hb_handle* h);
+/* LBM::EndIteration + SimulationState::Increment. */
+int hb_end_iteration(hb_handle* h);
+
+/* All phases of `n_steps` time steps; HB_STEP_MACRO fills the caches on the last. */
+int hb_step(hb_handle* h, int64_t n_steps, uint32_t flags);
+
+/* ---- state access ---------------------------------------------------------- */
+
+int hb_site_count(const hb_handle* h, int64_t* n);
+int hb_time_step(const hb_handle* h, uint64_t* t);          /* 1-based, as SimulationState */
+int hb_get_params(const hb_handle* h, hb_params* p);         /* LBM::GetLbmParams + iolets */
+/* f_old in reference order, AoS [n*19] (LatticeData::GetFOld after EndIteration). */
+int hb_get_fs(hb_handle* h, double* f);
+/* Replace f_old and f_new (InitialCondition / checkpoint restore). */
+int hb_set_fs(hb_handle* h, const double* f);
+/* MacroscopicPropertyCache of the last HB_STEP_MACRO step: density [n], velocity
+ * [n*3], wall-shear-stress magnitude [n] (NO_VALUE = DBL_MAX off the wall).
+ * Any pointer may be NULL. */
+int hb_get_macro(hb_handle* h, double* density, double* velocity, double* wss);
+/* Windkessel state of iolet `index` of `group` (0 inlets, 1 outlets):
+ * density, densityNew, flowRate, flowRateOld (InOutLetWK3 members). */
+int hb_get_wk3(hb_handle* h, int group, int index, double state[4]);
+
+/* Integer tables in reference order, for bit-exact comparison with the reference:
+ * neighbourIndices [n*19], wall and iolet masks [n], site type [n], iolet id [n],
+ * coords [n*3], per-type site counts [6] (any pointer may be NULL). */
+int hb_get_tables(const hb_handle* h, int64_t* neighbours, uint32_t* wall_mask, uint32_t* iolet_mask,
+                  int32_t* site_type, int32_t* iolet_id, int64_t* coords, int64_t* type_counts);
+
+/* ---- extraction and checkpoint (src/extraction/) ---------------------------- */
+
+/* Write one .xtr output step (LocalPropertyOutput::Write, float32 XDR) for the
+ * whole lattice with the listed fields ("velocity", "pressure", "shearstress",
+ * "distributions"; comma-separated).  Appends a record if the file exists with
+ * a matching header; `offset_path` (may be NULL) receives the .off file. */
+int hb_write_xtr(hb_handle* h, const char* path, const char* fields, const char* offset_path);
+/* Restore f from the "distributions" field of an .xtr at time step `step`
+ * (LocalDistributionInput::LoadDistribution). */
+int hb_read_checkpoint(hb_handle* h, const char* path, uint64_t step);
+
+/* ---- host-only readers (no GPU needed) ------------------------------------------ */
+
+/* SimConfig::DoIO for the collide-and-stream path: lattice-unit parameters and
+ * the geometry path (resolved against the case file's directory). */
+int hb_read_case(const char* xml_path, int kernel, hb_params* params, char* gmy_path, size_t gmy_path_len);
+
+typedef struct hb_geometry hb_geometry;
+/* GeometryReader + LatticeData on one rank: the reference-order tables. */
+int hb_geometry_open(const char* gmy_path, hb_geometry** out);
+int hb_geometry_site_count(const hb_geometry* g, int64_t* n, int64_t dims[3]);
+/* Same arrays as hb_get_tables plus wall distances [n*18] and normals [n*3]. */
+int hb_geometry_tables(const hb_geometry* g, int64_t* neighbours, uint32_t* wall_mask, uint32_t* iolet_mask,
+                       int32_t* site_type, int32_t* iolet_id, int64_t* coords, int64_t* type_counts,
+                       double* wall_distance, double* wall_normal);
+/* Device layout summary without allocating: run axis, runs, plain bulk sites,
+ * general sites (or an error if the lattice cannot be streamed exactly). */
+int hb_geometry_layout(const hb_geometry* g, const hb_params* params, int wall, int64_t stats[4]);
+int hb_geometry_close(hb_geometry* g);
+
+/* ---- measurement helpers ----------------------------------------------------- */
+
+/* Device-time of the last hb_step call's kernels in milliseconds (CUDA events),
+ * and the number of kernel launches it made. */
+int hb_last_step_timing(const hb_handle* h, double* ms, int64_t* launches);
+/* Advance `n_steps` steps with CUDA events around every launch (serialises the
+ * launches; for measurement only): ms[0] plain-bulk kernel, ms[1] boundary
+ * (general-site) kernel, ms[2] Windkessel kernel, summed over the steps. */
+int hb_profile_steps(hb_handle* h, int64_t n_steps, double ms[3]);
+/* Bytes of device memory held by the handle. */
+int hb_device_bytes(const hb_handle* h, int64_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HEMEB200_H */

@@ -90,7 +90,7 @@ class IoletCfg:
     density_mean: float = 0.0
     density_amp: float = 0.0
     phase: float = 0.0
-    period: float = 1.0
+    period: float = 0.0
     warmup: int = 0
     radius: float = 0.0
     max_speed: float = 0.0
