@@ -183,6 +183,12 @@ int hb_time_step(const hb_handle* h, uint64_t* t) {
   return HB_OK;
 }
 
+int hb_set_time_step(hb_handle* h, uint64_t t) {
+  if (!h || t == 0) return HB_ERR_ARG;
+  h->solver->set_time_step(t);
+  return HB_OK;
+}
+
 int hb_get_params(const hb_handle* h, hb_params* p) {
   if (!h || !p) return HB_ERR_ARG;
   *p = h->solver->params();

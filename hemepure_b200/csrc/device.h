@@ -10,6 +10,8 @@
 //   general    per general site (wall, iolet, or bulk sites whose neighbours do
 //              not follow the run pattern), structure of arrays, binned by
 //              collision type so a warp runs one streamer.
+//   ghost_a/b  [18][G] iolet ghost values (Nash / Ladd) of general site g for
+//              link d, ping-pong with f: slot inv(d) of the next step reads them.
 #pragma once
 
 #include <cstdint>
@@ -54,6 +56,8 @@ struct GeneralDev {
 struct StepArgs {
   const double* fin;
   double* fout;
+  const double* gin;      // iolet ghost values produced with fin [18][G]
+  double* gout;           // iolet ghost values of this step [18][G]
   int64_t np;
   int n;
   const int* meta;

@@ -12,11 +12,12 @@
 //   bounce-back     slot i = f*_{inv i}(x)            (SimpleBounceBackDelegate.h:36-44)
 //   BFL q >= 1/2    slot i = (f*_d + (2q-1) f*_i)/(2q), d = inv i
 //   BFL q <  1/2    slot i = 2q f*_d + (1-2q) slot_d  (the post-step, BouzidiFirdaousLallemandDelegate.h:54-93)
-//   Nash / Ladd     the ghost value is computed in the producing step and stored
-//                   in f*_d(x), which no neighbour reads (d points out of the domain)
+//   Nash / Ladd     the ghost value is computed in the producing step and kept in
+//                   a per-link ghost buffer (f*_d itself stays: the BFL rule of the
+//                   opposite wall link reads it)
 //   GZS             the virtual-node value is computed in the producing step
 //                   (reads the neighbour's pre-collision f by re-gathering it) and
-//                   stored in f*_d(x) likewise.
+//                   stored in f*_d(x), which nothing else reads (d points into the wall).
 #include <cuda_runtime.h>
 
 #include "device.h"
@@ -173,7 +174,7 @@ __device__ __forceinline__ void gather_general(const StepArgs& a, int g, int s, 
     const int d = inv(i);
     const bool bw = (wm >> (d - 1)) & 1u, bi = (im >> (d - 1)) & 1u;
     if (bi) {
-      f[i] = ld(a.fin + (int64_t)d * a.np + s);
+      f[i] = ld(a.gin + (int64_t)(d - 1) * G.G + g);
     } else if (bw) {
       if (WALL == kBFL) {
         const double q = (double)__ldg(G.q + (int64_t)(d - 1) * G.G + g);
@@ -317,14 +318,14 @@ __global__ void __launch_bounds__(128) k_general(const StepArgs a) {
         w[1] *= rho;
         w[2] *= rho;
         const double corr = 2. * weight(d) * (w[0] * cx(d) + w[1] * cy(d) + w[2] * cz(d)) / kCs2;
-        out[d] = fp[d] - corr;
+        a.gout[(int64_t)(d - 1) * G.G + g] = fp[d] - corr;
       } else {
         // NashZerothOrderPressureDelegate::StreamLink (src/lb/streamers/NashZerothOrderPressureDelegate.h:36-76).
         const double rb = a.dens_row[io];
         const double nx = I.nrm_f[0], ny = I.nrm_f[1], nz = I.nrm_f[2];
         const double comp = (mx / rho) * nx + (my / rho) * ny + (mz / rho) * nz;
         const FeqConst gq(rb, nx * comp * rb, ny * comp * rb, nz * comp * rb);
-        out[d] = gq(inv(d));
+        a.gout[(int64_t)(d - 1) * G.G + g] = gq(inv(d));
       }
     }
   }

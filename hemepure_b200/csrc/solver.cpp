@@ -109,6 +109,11 @@ void Solver::upload() {
     tot += (int64_t)f_[b].bytes;
     check(cudaMemset(f_[b].p, 0, f_[b].bytes), "cudaMemset");
   }
+  for (int b = 0; b < 2; b++) {
+    ghost_[b].alloc((size_t)18 * std::max(1, L_.G) * sizeof(double));
+    tot += (int64_t)ghost_[b].bytes;
+    check(cudaMemset(ghost_[b].p, 0, ghost_[b].bytes), "cudaMemset");
+  }
   upload_vec(meta_, L_.meta, tot);
   upload_vec(run_off_, L_.run_off, tot);
   upload_vec(st2ref_, L_.st2ref, tot);
@@ -218,6 +223,8 @@ StepArgs Solver::args() const {
   std::memset(&a, 0, sizeof(a));
   a.fin = f_[cur_].as<double>();
   a.fout = f_[1 - cur_].as<double>();
+  a.gin = ghost_[cur_].as<double>();
+  a.gout = ghost_[1 - cur_].as<double>();
   a.np = L_.np;
   a.n = L_.n;
   a.meta = meta_.as<int>();
@@ -406,6 +413,7 @@ bool Solver::get_previous_fs(double* f) {
   tmp.alloc((size_t)L_.n * Q * sizeof(double));
   StepArgs a = args();
   a.fin = f_[1 - cur_].as<double>();
+  a.gin = ghost_[1 - cur_].as<double>();
   if (prev_direct_) {
     launch_soa_to_aos_f64(a.fin, L_.np, st2ref_.as<int>(), L_.n, tmp.as<double>(), stream_);
   } else {

@@ -82,6 +82,7 @@ class Solver {
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
 
   DeviceBuffer f_[2];
+  DeviceBuffer ghost_[2];         // iolet ghost values, paired with f_
   int cur_ = 0;
   bool direct_ = true;            // f_[cur_] holds pre-collision f (else post-collision f*)
   DeviceBuffer meta_, run_off_, st2ref_;

@@ -38,6 +38,7 @@ EXPORTS = [
     "hb_get_macro", "hb_get_wk3", "hb_get_tables", "hb_write_xtr", "hb_read_checkpoint",
     "hb_last_step_timing", "hb_device_bytes", "hb_read_case", "hb_geometry_open", "hb_geometry_site_count",
     "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_close", "hb_profile_steps",
+    "hb_set_time_step",
 ]
 
 
@@ -118,6 +119,7 @@ def library() -> C.CDLL:
     L.hb_geometry_layout.argtypes = [P, P, I, P]
     L.hb_geometry_close.argtypes = [P]
     L.hb_profile_steps.argtypes = [P, I64, P]
+    L.hb_set_time_step.argtypes = [P, U64]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name != "hb_default_options":
@@ -228,6 +230,10 @@ class LBM:
         t = C.c_uint64()
         library().hb_time_step(self._h, C.byref(t))
         return int(t.value)
+
+    @time_step.setter
+    def time_step(self, t: int) -> None:
+        self._check(library().hb_set_time_step(self._h, int(t)))
 
     def GetLbmParams(self) -> Params:
         p = Params()

@@ -571,13 +571,22 @@ def make_case(name: str, out_dir: str, steps: Optional[int] = None, scale: float
         # inlet (mean 1, amplitude 1e-3, period 4000), two WK3 outlets.
         v = YBifurcation(sc(32), sc(400, 8), sc(25), sc(400, 8), 35.0)
         u = CaseUnits(tau=0.52)
+        # Windkessel sizing.  The reference integrates the absolute lattice pressure
+        # (InOutLetWK3.cc:72-91), so the total resistance must carry the outlet at
+        # p = cs^2 rho with rho ~ 1 for the Poiseuille flow the branches admit; the
+        # characteristic resistance is the lattice wave impedance cs/A (a larger one
+        # makes the one-step-lagged flow feedback unstable); C gives R_p C ~ 2000 steps.
+        mu = (u.tau - 0.5) / 3.0
+        r_par = 8.0 * mu * v.lp / (math.pi * v.rp ** 4)
+        r_dau = 8.0 * mu * v.ld / (math.pi * v.rd ** 4)
+        q_out = CS2 * 5e-4 / (2.0 * r_par + r_dau)
+        area = math.pi * v.rd ** 2
         outs = []
         for _ in range(2):
-            rp = float(rng.uniform(0.5, 1.5)) * 1e-3
-            cp = 2000.0 / rp
-            rc = 0.1 * rp
-            area = math.pi * v.rd ** 2
-            outs.append(WK3BC(r_c=rc, r_p=rp, c_p=cp, area=area))
+            r_tot = CS2 / q_out * float(rng.uniform(0.8, 1.2))
+            rc = math.sqrt(CS2) / area
+            rp = r_tot - rc
+            outs.append(WK3BC(r_c=rc, r_p=rp, c_p=2000.0 / rp, area=area))
         write_case_xml(xml, os.path.basename(gmy), v, u, steps or 8000,
                        [PressureBC(1.0, 1e-3, 4000.0)], outs, relaxation_parameter=3.0 / 16.0)
     elif name == "stenosis":

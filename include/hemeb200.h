@@ -150,6 +150,8 @@ int hb_step(hb_handle* h, int64_t n_steps, uint32_t flags);
 
 int hb_site_count(const hb_handle* h, int64_t* n);
 int hb_time_step(const hb_handle* h, uint64_t* t);          /* 1-based, as SimulationState */
+/* Set the time step of the next step (InitialCondition::SetTime, src/lb/InitialCondition.cc:18-21). */
+int hb_set_time_step(hb_handle* h, uint64_t t);
 int hb_get_params(const hb_handle* h, hb_params* p);         /* LBM::GetLbmParams + iolets */
 /* f_old in reference order, AoS [n*19] (LatticeData::GetFOld after EndIteration). */
 int hb_get_fs(hb_handle* h, double* f);

@@ -1,0 +1,45 @@
+"""Regenerate the golden fixtures under tests/golden/ from the reference tree.
+
+Run in a container where the reference is mounted (its path is the first
+argument, default /root/reference).  It copies the reference's own 380-byte
+unit-test geometry (src/unittests/resources/four_cube.gmy) and records, for the
+geometries shipped with the reference's example cases, the site counts and
+table checksums that the oracle reads from them.
+"""
+
+import hashlib
+import json
+import os
+import shutil
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import oracle as O  # noqa: E402
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+CASES = ["cases/pipe/pipe.gmy", "cases/bifurcation/bifurcation_lores/bifurcation.gmy",
+         "cases/FiveExit/SixBranch.gmy", "cases/UnevenArms/UnevenArms.gmy", "cases/elasticWallsExample/pipe.gmy"]
+
+
+def sha(a):
+    return hashlib.sha256(a.tobytes()).hexdigest()
+
+
+def main():
+    src = os.path.join(REF, "src/unittests/resources/four_cube.gmy")
+    shutil.copyfile(src, os.path.join(HERE, "four_cube.gmy"))
+    out = {}
+    for rel in CASES:
+        lat = O.Lattice(os.path.join(REF, rel))
+        w, io, t, i = lat.sitedata()
+        out[rel] = {"sites": lat.n, "type_counts": lat.type_counts().tolist(),
+                    "sha256_neighbours": sha(lat.neighbours()), "sha256_coords": sha(lat.coords()),
+                    "sha256_wall_mask": sha(w), "sha256_iolet_mask": sha(io)}
+    with open(os.path.join(HERE, "reference_geometries.json"), "w") as fh:
+        json.dump(out, fh, indent=1)
+
+
+if __name__ == "__main__":
+    main()

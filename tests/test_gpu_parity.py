@@ -80,6 +80,7 @@ def test_get_set_fs_round_trip(case_dir):
     assert np.array_equal(a.GetFOld(), b.GetFOld())
     c = lbm.LBM(xml, kernel=kernel, wall=wall)
     c.SetFs(mid)
+    c.time_step = 8
     c.step(6)
     assert np.array_equal(c.GetFOld(), b.GetFOld())
 
