@@ -433,23 +433,29 @@ __global__ void __launch_bounds__(256) k_gather_aos(const StepArgs a, const int*
   for (int i = 0; i < Q; i++) aos[base + i] = f[i];
 }
 
+// One block per Windkessel iolet.  The flow-rate sum runs in the reference's
+// order (sites in contiguous order, one add after another, InOutLetWK3.cc:95):
+// the block stages the contributions in shared memory with coalesced loads and
+// thread 0 adds them in sequence, so the outlet density is bit-identical.
 __global__ void k_wk3_begin(WK3Dev* wk3, const double* cpl_buf, double* dens_row) {
-  __shared__ double part[256];
+  constexpr int kChunk = 2048;
+  __shared__ double stage[kChunk];
   WK3Dev& W = wk3[blockIdx.x];
   const int n = W.count_prev;
   double acc = 0.0;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) acc += cpl_buf[W.cpl_start + k];
-  part[threadIdx.x] = acc;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) part[threadIdx.x] = part[threadIdx.x] + part[threadIdx.x + w];
+  for (int base = 0; base < n; base += kChunk) {
+    const int m = min(kChunk, n - base);
+    for (int k = threadIdx.x; k < m; k += blockDim.x) stage[k] = cpl_buf[W.cpl_start + base + k];
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int k = 0; k < m; k++) acc = acc + stage[k];
     __syncthreads();
   }
   if (threadIdx.x == 0) {
     // InOutLetWK3::DoComms (self-message on one rank), then the centre site's
     // DoPreStreamCoupling and DoPostStreamCoupling (InOutLetWK3.cc:33-105).
     const double density = W.density_new;
-    double flow = part[0];
+    double flow = 0.0 + acc;
     if (n != 0) flow = flow * W.area / (double)n;
     dens_row[W.iolet] = density;
     double d_after = density, flow_old = W.flow_old;

@@ -88,15 +88,22 @@ Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& 
     omega_minus_ = -1.0 / tau_minus;
   }
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
   check(cudaEventCreate(&ev0_), "cudaEventCreate");
   check(cudaEventCreate(&ev1_), "cudaEventCreate");
+  check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
+  check(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "cudaEventCreate");
   upload();
 }
 
 Solver::~Solver() {
   if (stream_) cudaStreamSynchronize(stream_);
+  if (side_) cudaStreamSynchronize(side_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
+  if (fork_) cudaEventDestroy(fork_);
+  if (join_) cudaEventDestroy(join_);
+  if (side_) cudaStreamDestroy(side_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -300,7 +307,19 @@ void Solver::request_comms() {
 void Solver::pre_receive(bool macro, int which) {
   if (!phase_open_) request_comms();
   if (macro) ensure_macro();
-  launch_step_f64(args(), opt_.kernel, opt_.wall, !direct_, macro, which, 256, 128, stream_);
+  const StepArgs a = args();
+  if (which == 3 && L_.G > 0) {
+    // The boundary kernel (general sites) is latency-bound and the bulk kernel
+    // bandwidth-bound: run them side by side, both after the Windkessel update.
+    check(cudaEventRecord(fork_, stream_), "fork");
+    check(cudaStreamWaitEvent(side_, fork_, 0), "fork");
+    launch_step_f64(a, opt_.kernel, opt_.wall, !direct_, macro, 2, 256, 128, side_);
+    check(cudaEventRecord(join_, side_), "join");
+    launch_step_f64(a, opt_.kernel, opt_.wall, !direct_, macro, 1, 256, 128, stream_);
+    check(cudaStreamWaitEvent(stream_, join_, 0), "join");
+  } else {
+    launch_step_f64(a, opt_.kernel, opt_.wall, !direct_, macro, which, 256, 128, stream_);
+  }
   check(cudaGetLastError(), "step kernel launch");
   phase_macro_ = macro;
 }

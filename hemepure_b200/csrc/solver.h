@@ -79,7 +79,9 @@ class Solver {
   hb_options opt_;
   Layout L_;
   cudaStream_t stream_ = nullptr;
+  cudaStream_t side_ = nullptr;   // boundary kernel, concurrent with the bulk kernel
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaEvent_t fork_ = nullptr, join_ = nullptr;
 
   DeviceBuffer f_[2];
   DeviceBuffer ghost_[2];         // iolet ghost values, paired with f_
