@@ -255,6 +255,24 @@ def main():
            "d2h_bytes_per_step": 4, "steps": e2e_steps,
            "note": "one hb_step(1) call per step: iolet densities up, stability word down, host sync"}
 
+    # The shifted low-precision forms on the same lattice (same step count).
+    forms = {"fp64": {"MLUPS": value / world, "bytes_per_site": 304,
+                      "whole_step_frac": roofline["whole_step_frac"]}}
+    for prec, nbytes in (("fp32", 152), ("fp16", 76)):
+        try:
+            ms_p = lbm.LBM(xml, kernel=kernel, wall=wall, precision=prec, device=local)
+            ms_p.step(warmup)
+            ms_p.step(args.steps)
+            t_ms, _ = ms_p.last_step_timing()
+            b_p, g_p, _ = ms_p.profile_steps(prof_steps)
+            ms_p.close()
+            per = t_ms / args.steps
+            forms[prec] = {"MLUPS": n_sites / (per * 1e-3) / 1e6, "ms_per_step": per, "bytes_per_site": nbytes,
+                           "whole_step_frac": nbytes * n_sites / (per * 1e-3) / 1e9 / peak,
+                           "bulk_kernel_GBs": nbytes * lay["bulk_sites"] / (b_p / prof_steps * 1e-3) / 1e9}
+        except Exception as e:  # report, do not hide
+            forms[prec] = {"error": str(e)}
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(xml, kernel, wall, n_sites)
@@ -263,7 +281,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
                 "warmup": warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
-                "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "clocks": clocks,
+                "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "clocks": clocks, "forms": forms,
                 "gpu_launches": int(launches), "wall_s": wall_s}
         print(json.dumps(line), flush=True)
     sim.close()

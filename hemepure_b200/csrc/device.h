@@ -43,9 +43,10 @@ struct WK3Dev {           // InOutLetWK3 state
 struct GeneralDev {
   int G;
   const int* site;        // [G] storage index
+  const int* run;         // [G] run whose offsets the bulk slots follow, or -1
   const uint32_t* wall;   // [G] wall-link mask (bit d-1 for direction d)
   const uint32_t* iolet;  // [G] iolet-link mask
-  const int* src;         // [18][G] pull source of slots 1..18 (own index for boundary slots)
+  const int* src;         // [18][G] pull source of slots 1..18 when run < 0
   const float* q;         // [18][G] wall distances (BFL, GZS)
   const float* nrm;       // [3][G] wall normal (float, normalised in float)
   const int* io;          // [G] iolet table index or -1
@@ -88,6 +89,15 @@ void launch_gather_f64(const StepArgs& a, int wall, void* stream);
 void launch_gather_aos_f64(const StepArgs& a, int wall, const int* st2ref, double* aos, void* stream);
 void launch_wk3_begin(WK3Dev* wk3, int nwk3, const double* cpl_buf, double* dens_row, void* stream);
 void launch_equilibrium_f64(double* f, int64_t np, int n, const double feq[19], void* stream);
+void launch_equilibrium_aos_f64(double* f, int n, const double feq[19], void* stream);
+// Shifted low-precision storage (kernels_mixed.cu): g = f - w stored as FP32, or
+// as FP16 scaled by 1/inv_scale; ghosts in FP32.
+void launch_step_mixed(const StepArgs& a, int precision, const void* fin, void* fout, const float* gin, float* gout,
+                       float inv_scale, int kernel, int wall, bool gather, bool macro, int which, void* stream);
+void launch_to_aos_mixed(const StepArgs& a, int precision, const void* fin, const float* gin, float inv_scale, int wall,
+                         bool gather, const int* st2ref, double* aos, void* stream);
+void launch_from_aos_mixed(const double* aos, const int* st2ref, int n, int64_t np, int precision, void* out,
+                           float inv_scale, void* stream);
 // AoS reference order <-> SoA storage order.
 void launch_soa_to_aos_f64(const double* soa, int64_t np, const int* st2ref, int n, double* aos, void* stream);
 void launch_aos_to_soa_f64(const double* aos, const int* st2ref, int n, double* soa, int64_t np, void* stream);

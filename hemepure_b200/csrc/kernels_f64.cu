@@ -147,9 +147,19 @@ __device__ __forceinline__ bool parabolic(const IoletDev& I, const double x[3], 
 __device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
 
 // Pre-collision f of a plain bulk site.
+__device__ __forceinline__ void load_run_offsets(const StepArgs& a, int r, int* off);
+
 __device__ __forceinline__ void gather_bulk(const StepArgs& a, int s, int r, double* f) {
-  const int4* o4 = reinterpret_cast<const int4*>(a.run_off) + 5 * r;
   int off[20];
+  load_run_offsets(a, r, off);
+  f[0] = ld(a.fin + s);
+#pragma unroll
+  for (int i = 1; i < Q; i++) f[i] = ld(a.fin + (int64_t)i * a.np + (s + off[i]));
+}
+
+// Pre-collision f of general site g (rules above).
+__device__ __forceinline__ void load_run_offsets(const StepArgs& a, int r, int* off) {
+  const int4* o4 = reinterpret_cast<const int4*>(a.run_off) + 5 * r;
 #pragma unroll
   for (int k = 0; k < 5; k++) {
     const int4 v = __ldg(o4 + k);
@@ -158,16 +168,15 @@ __device__ __forceinline__ void gather_bulk(const StepArgs& a, int s, int r, dou
     off[4 * k + 2] = v.z;
     off[4 * k + 3] = v.w;
   }
-  f[0] = ld(a.fin + s);
-#pragma unroll
-  for (int i = 1; i < Q; i++) f[i] = ld(a.fin + (int64_t)i * a.np + (s + off[i]));
 }
 
-// Pre-collision f of general site g (rules above).
 template <int WALL>
 __device__ __forceinline__ void gather_general(const StepArgs& a, int g, int s, double* f) {
   const GeneralDev& G = a.gen;
   const uint32_t wm = __ldg(G.wall + g), im = __ldg(G.iolet + g);
+  const int run = __ldg(G.run + g);
+  int off[20];
+  if (run >= 0) load_run_offsets(a, run, off);
   f[0] = ld(a.fin + s);
 #pragma unroll
   for (int i = 1; i < Q; i++) {
@@ -186,7 +195,7 @@ __device__ __forceinline__ void gather_general(const StepArgs& a, int g, int s, 
         f[i] = ld(a.fin + (int64_t)d * a.np + s);
       }
     } else {
-      const int src = __ldg(G.src + (int64_t)(i - 1) * G.G + g);
+      const int src = run >= 0 ? s + off[i] : __ldg(G.src + (int64_t)(i - 1) * G.G + g);
       f[i] = ld(a.fin + (int64_t)i * a.np + src);
     }
   }
@@ -360,7 +369,8 @@ __global__ void __launch_bounds__(128) k_general(const StepArgs a) {
         } else if ((wm >> (i - 1)) & 1u) {
           sbb = true;
         } else {
-          const int nb = __ldg(G.src + (int64_t)(d - 1) * G.G + g);
+          const int grun = __ldg(G.run + g);
+          const int nb = grun >= 0 ? s + __ldg(a.run_off + 20 * grun + d) : __ldg(G.src + (int64_t)(d - 1) * G.G + g);
           double fn[Q];
           gather_any<WALL, GATHER>(a, nb, fn);
           double rn, mnx, mny, mnz;
@@ -478,11 +488,12 @@ struct Row19 {
   double v[Q];
 };
 
-__global__ void k_fill(double* f, int64_t np, int n, Row19 row) {
+// f[i*dir_stride + s*site_stride] = row[i]: SoA with (np, 1), AoS with (1, 19).
+__global__ void k_fill(double* f, int64_t dir_stride, int64_t site_stride, int n, Row19 row) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
 #pragma unroll
-  for (int i = 0; i < Q; i++) f[(int64_t)i * np + s] = row.v[i];
+  for (int i = 0; i < Q; i++) f[(int64_t)i * dir_stride + (int64_t)s * site_stride] = row.v[i];
 }
 
 __global__ void k_soa_to_aos(const double* soa, int64_t np, const int* st2ref, int n, double* aos) {
@@ -558,7 +569,13 @@ void launch_wk3_begin(WK3Dev* wk3, int nwk3, const double* cpl_buf, double* dens
 void launch_equilibrium_f64(double* f, int64_t np, int n, const double feq[19], void* stream) {
   Row19 r;
   for (int i = 0; i < Q; i++) r.v[i] = feq[i];
-  if (n > 0) k_fill<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(f, np, n, r);
+  if (n > 0) k_fill<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(f, np, 1, n, r);
+}
+
+void launch_equilibrium_aos_f64(double* f, int n, const double feq[19], void* stream) {
+  Row19 r;
+  for (int i = 0; i < Q; i++) r.v[i] = feq[i];
+  if (n > 0) k_fill<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(f, 1, Q, n, r);
 }
 
 void launch_soa_to_aos_f64(const double* soa, int64_t np, const int* st2ref, int n, double* aos, void* stream) {

@@ -129,27 +129,34 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
                                                       : "a distribution slot is written twice in a step (inconsistent cut links)"};
   }
 
-  // Run offsets: taken from the first site of each run whose slots are all bulk.
+  // Run offsets, per direction: from the first site of the run whose slot is a
+  // bulk pull.  A site follows its run when every bulk slot matches them.
   L.run_off.assign((size_t)runs * 20, 0);
-  std::vector<char> run_set(runs, 0);
+  std::vector<uint32_t> run_set(runs, 0u);
   L.meta.assign(n, 0);
-  std::vector<char> plain(n, 0);
+  std::vector<char> plain(n, 0), regular(n, 0);
   for (int s = 0; s < n; s++) {
-    const int x = L.st2ref[s];
-    if (t.collision_type(x) != 0) continue;
-    bool all_bulk = true;
-    for (int i = 1; i < Q; i++)
-      if (src[(size_t)s * Q + i] < 0) all_bulk = false;
-    if (!all_bulk) continue;
     const int r = run_of[s];
     int* off = &L.run_off[(size_t)r * 20];
-    if (!run_set[r]) {
-      for (int i = 1; i < Q; i++) off[i] = src[(size_t)s * Q + i] - s;
-      run_set[r] = 1;
+    for (int i = 1; i < Q; i++) {
+      const int v = src[(size_t)s * Q + i];
+      if (v >= 0 && !((run_set[r] >> i) & 1u)) {
+        off[i] = v - s;
+        run_set[r] |= 1u << i;
+      }
     }
-    bool ok = src[(size_t)s * Q] == s;
-    for (int i = 1; i < Q && ok; i++) ok = (src[(size_t)s * Q + i] - s) == off[i];
-    if (ok) plain[s] = 1;
+  }
+  for (int s = 0; s < n; s++) {
+    const int r = run_of[s];
+    const int* off = &L.run_off[(size_t)r * 20];
+    bool ok = src[(size_t)s * Q] == s, all_bulk = true;
+    for (int i = 1; i < Q; i++) {
+      const int v = src[(size_t)s * Q + i];
+      if (v < 0) all_bulk = false;
+      else if (v - s != off[i]) ok = false;
+    }
+    regular[s] = ok;
+    plain[s] = ok && all_bulk && t.collision_type(L.st2ref[s]) == 0;
   }
 
   // General sites, binned by collision type.
@@ -162,6 +169,7 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
   L.bulk_sites = n - G;
   for (int s = 0; s < n; s++) L.meta[s] = plain[s] ? run_of[s] : 0;
   L.g_site.resize(G);
+  L.g_run.resize(G);
   L.g_src.resize((size_t)18 * G);
   L.g_io.assign(G, -1);
   L.g_cpl.assign(G, -1);
@@ -185,6 +193,8 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
     const int x = L.st2ref[s];
     L.meta[s] = -(g + 1);
     L.g_site[g] = s;
+    L.g_run[g] = regular[s] ? run_of[s] : -1;
+    if (regular[s]) L.regular_general++;
     const int ct = t.collision_type(x);
     L.g_kind[g] = ct;
     L.kind_start[ct + 1]++;

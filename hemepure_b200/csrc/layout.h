@@ -21,7 +21,8 @@ struct Layout {
   int bulk_sites = 0;
   // general sites (structure of arrays)
   int G = 0;
-  std::vector<int> g_site, g_src, g_io, g_cpl, g_xyz, g_kind;
+  std::vector<int> g_site, g_run, g_src, g_io, g_cpl, g_xyz, g_kind;
+  int regular_general = 0;        // general sites whose bulk slots follow their run
   std::vector<uint32_t> g_wall, g_iolet;
   std::vector<float> g_q, g_nrm;
   int kind_start[7] = {0, 0, 0, 0, 0, 0, 0};   // bins by collision type

@@ -69,7 +69,8 @@ void upload_vec(DeviceBuffer& b, const std::vector<T>& v, int64_t& total) {
 Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& opt)
     : t_(std::move(tables)), p_(params), opt_(opt) {
   if (opt_.kernel < 0 || opt_.kernel > 2 || opt_.wall < 0 || opt_.wall > 2) throw Error{HB_ERR_ARG, "unknown kernel or wall type"};
-  if (opt_.precision != HB_STORE_FP64) throw Error{HB_ERR_UNSUPPORTED, "this handle type stores FP64 distributions"};
+  if (opt_.precision < HB_STORE_FP64 || opt_.precision > HB_STORE_FP16) throw Error{HB_ERR_ARG, "unknown storage precision"};
+  inv_scale_ = opt_.precision == HB_STORE_FP16 ? 1.0f / 1024.0f : 1.0f;
   if (opt_.kernel == kLES && opt_.wall == kGZS)
     throw Error{HB_ERR_UNSUPPORTED, "GZS walls with the LES kernel: the virtual-node collision has no relaxation time"};
   if (!(p_.tau > 0.5)) throw Error{HB_ERR_ARG, "tau must exceed 1/2"};
@@ -112,12 +113,12 @@ void Solver::upload() {
   const int64_t np = L_.np;
   int64_t tot = 0;
   for (int b = 0; b < 2; b++) {
-    f_[b].alloc((size_t)Q * np * sizeof(double));
+    f_[b].alloc((size_t)Q * np * elem_bytes());
     tot += (int64_t)f_[b].bytes;
     check(cudaMemset(f_[b].p, 0, f_[b].bytes), "cudaMemset");
   }
   for (int b = 0; b < 2; b++) {
-    ghost_[b].alloc((size_t)18 * std::max(1, L_.G) * sizeof(double));
+    ghost_[b].alloc((size_t)18 * std::max(1, L_.G) * (mixed() ? sizeof(float) : sizeof(double)));
     tot += (int64_t)ghost_[b].bytes;
     check(cudaMemset(ghost_[b].p, 0, ghost_[b].bytes), "cudaMemset");
   }
@@ -125,6 +126,7 @@ void Solver::upload() {
   upload_vec(run_off_, L_.run_off, tot);
   upload_vec(st2ref_, L_.st2ref, tot);
   upload_vec(g_site_, L_.g_site, tot);
+  upload_vec(g_run_, L_.g_run, tot);
   upload_vec(g_wall_, L_.g_wall, tot);
   upload_vec(g_iolet_, L_.g_iolet, tot);
   upload_vec(g_src_, L_.g_src, tot);
@@ -210,7 +212,16 @@ void Solver::upload() {
   // Equilibrium initial condition in direct form.
   double feq[Q];
   feq_host(p_.initial_density, 0.0, 0.0, 0.0, feq);
-  launch_equilibrium_f64(f_[0].as<double>(), np, n, feq, stream_);
+  if (!mixed()) {
+    launch_equilibrium_f64(f_[0].as<double>(), np, n, feq, stream_);
+  } else {
+    // The equilibrium filled in FP64 AoS on the device, then shifted and narrowed.
+    DeviceBuffer aos;
+    aos.alloc((size_t)n * Q * sizeof(double));
+    launch_equilibrium_aos_f64(aos.as<double>(), n, feq, stream_);
+    launch_from_aos_mixed(aos.as<double>(), st2ref_.as<int>(), n, np, opt_.precision, f_[0].p, inv_scale_, stream_);
+    check(cudaStreamSynchronize(stream_), "initialisation");
+  }
   check(cudaGetLastError(), "equilibrium fill");
   cur_ = 0;
   direct_ = true;
@@ -238,6 +249,7 @@ StepArgs Solver::args() const {
   a.run_off = run_off_.as<int>();
   a.gen.G = L_.G;
   a.gen.site = g_site_.as<int>();
+  a.gen.run = g_run_.as<int>();
   a.gen.wall = g_wall_.as<uint32_t>();
   a.gen.iolet = g_iolet_.as<uint32_t>();
   a.gen.src = g_src_.as<int>();
@@ -313,15 +325,35 @@ void Solver::pre_receive(bool macro, int which) {
     // bandwidth-bound: run them side by side, both after the Windkessel update.
     check(cudaEventRecord(fork_, stream_), "fork");
     check(cudaStreamWaitEvent(side_, fork_, 0), "fork");
-    launch_step_f64(a, opt_.kernel, opt_.wall, !direct_, macro, 2, 256, 128, side_);
+    launch(a, macro, 2, side_);
     check(cudaEventRecord(join_, side_), "join");
-    launch_step_f64(a, opt_.kernel, opt_.wall, !direct_, macro, 1, 256, 128, stream_);
+    launch(a, macro, 1, stream_);
     check(cudaStreamWaitEvent(stream_, join_, 0), "join");
   } else {
-    launch_step_f64(a, opt_.kernel, opt_.wall, !direct_, macro, which, 256, 128, stream_);
+    launch(a, macro, which, stream_);
   }
   check(cudaGetLastError(), "step kernel launch");
   phase_macro_ = macro;
+}
+
+void Solver::launch(const StepArgs& a, bool macro, int which, cudaStream_t st) {
+  if (!mixed()) {
+    launch_step_f64(a, opt_.kernel, opt_.wall, !direct_, macro, which, 256, 128, st);
+  } else {
+    launch_step_mixed(a, opt_.precision, f_[cur_].p, f_[1 - cur_].p, ghost_[cur_].as<float>(), ghost_[1 - cur_].as<float>(),
+                      inv_scale_, opt_.kernel, opt_.wall, !direct_, macro, which, st);
+  }
+}
+
+// Pre-collision f in FP64 AoS reference order: the current state (use_prev false)
+// or the state that entered the last completed step (use_prev true).
+void Solver::to_aos(bool use_prev, double* dev_aos) {
+  StepArgs a = args();
+  const int b = use_prev ? 1 - cur_ : cur_;
+  const bool gather = use_prev ? !prev_direct_ : !direct_;
+  launch_to_aos_mixed(a, opt_.precision, f_[b].p, ghost_[b].as<float>(), inv_scale_, opt_.wall, gather, st2ref_.as<int>(),
+                      dev_aos, stream_);
+  check(cudaGetLastError(), "to_aos launch");
 }
 
 void Solver::end_iteration() {
@@ -430,6 +462,12 @@ bool Solver::get_previous_fs(double* f) {
   if (!prev_valid_) return false;
   DeviceBuffer tmp;
   tmp.alloc((size_t)L_.n * Q * sizeof(double));
+  if (mixed()) {
+    to_aos(true, tmp.as<double>());
+    check(cudaMemcpyAsync(f, tmp.p, (size_t)L_.n * Q * sizeof(double), cudaMemcpyDeviceToHost, stream_), "f download");
+    check(cudaStreamSynchronize(stream_), "get_previous_fs");
+    return true;
+  }
   StepArgs a = args();
   a.fin = f_[1 - cur_].as<double>();
   a.gin = ghost_[1 - cur_].as<double>();
@@ -451,6 +489,14 @@ void Solver::set_units(double dt, double dx, const double origin[3]) {
 }
 
 void Solver::get_fs(double* f) {
+  if (mixed()) {
+    DeviceBuffer tmp;
+    tmp.alloc((size_t)L_.n * Q * sizeof(double));
+    to_aos(false, tmp.as<double>());
+    check(cudaMemcpyAsync(f, tmp.p, (size_t)L_.n * Q * sizeof(double), cudaMemcpyDeviceToHost, stream_), "f download");
+    check(cudaStreamSynchronize(stream_), "get_fs");
+    return;
+  }
   materialise();
   double* aos = f_[1 - cur_].as<double>();  // the spare buffer holds n*19 doubles
   launch_soa_to_aos_f64(f_[cur_].as<double>(), L_.np, st2ref_.as<int>(), L_.n, aos, stream_);
@@ -460,6 +506,17 @@ void Solver::get_fs(double* f) {
 }
 
 void Solver::set_fs(const double* f) {
+  if (mixed()) {
+    DeviceBuffer tmp;
+    tmp.alloc((size_t)L_.n * Q * sizeof(double));
+    check(cudaMemcpyAsync(tmp.p, f, (size_t)L_.n * Q * sizeof(double), cudaMemcpyHostToDevice, stream_), "f upload");
+    launch_from_aos_mixed(tmp.as<double>(), st2ref_.as<int>(), L_.n, L_.np, opt_.precision, f_[cur_].p, inv_scale_, stream_);
+    check(cudaGetLastError(), "from_aos launch");
+    direct_ = true;
+    prev_valid_ = false;
+    check(cudaStreamSynchronize(stream_), "set_fs");
+    return;
+  }
   double* aos = f_[1 - cur_].as<double>();
   check(cudaMemcpyAsync(aos, f, (size_t)L_.n * Q * sizeof(double), cudaMemcpyHostToDevice, stream_), "f upload");
   launch_aos_to_soa_f64(aos, st2ref_.as<int>(), L_.n, f_[cur_].as<double>(), L_.np, stream_);

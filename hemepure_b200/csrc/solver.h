@@ -73,6 +73,10 @@ class Solver {
   void fill_density_rows(uint64_t t_first, int count);
   StepArgs args() const;
   void check(cudaError_t e, const char* what);
+  bool mixed() const { return opt_.precision != HB_STORE_FP64; }
+  size_t elem_bytes() const { return opt_.precision == HB_STORE_FP64 ? 8 : (opt_.precision == HB_STORE_FP32 ? 4 : 2); }
+  void launch(const StepArgs& a, bool macro, int which, cudaStream_t st);
+  void to_aos(bool use_prev, double* dev_aos);
 
   LatticeTables t_;
   hb_params p_;
@@ -88,6 +92,7 @@ class Solver {
   int cur_ = 0;
   bool direct_ = true;            // f_[cur_] holds pre-collision f (else post-collision f*)
   DeviceBuffer meta_, run_off_, st2ref_;
+  DeviceBuffer g_run_;
   DeviceBuffer g_site_, g_wall_, g_iolet_, g_src_, g_q_, g_nrm_, g_io_, g_cpl_, g_xyz_;
   DeviceBuffer vtau_, iolets_, dens_, cpl_buf_, wk3_, status_;
   DeviceBuffer rho_, u_, wss_;
@@ -104,6 +109,7 @@ class Solver {
   int64_t last_launches_ = 0;
   int64_t dev_bytes_ = 0;
   int status_sticky_ = 0;
+  float inv_scale_ = 1.0f;        // FP16 storage holds g / inv_scale
   bool prev_valid_ = false;
   bool prev_direct_ = false;
   double dt_ = 1.0, dx_ = 1.0;
