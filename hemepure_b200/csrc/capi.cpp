@@ -50,6 +50,11 @@ int finish_create(hb::LatticeTables t, const hb_params& p, const hb_options& o, 
 
 }  // namespace
 
+namespace hb {
+// Message for hb_last_error(NULL, ...) from entry points that take no handle.
+void set_last_error(const std::string& msg) { g_create_error = msg; }
+}  // namespace hb
+
 extern "C" {
 
 void hb_default_options(hb_options* opt) {
@@ -215,6 +220,14 @@ int hb_get_macro(hb_handle* h, double* density, double* velocity, double* wss) {
   if (!h) return HB_ERR_ARG;
   return guard(h, [&] {
     h->solver->get_macro(density, velocity, wss);
+    return HB_OK;
+  });
+}
+
+int hb_moment_sums(hb_handle* h, double sums[4]) {
+  if (!h || !sums) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->moment_sums(sums);
     return HB_OK;
   });
 }

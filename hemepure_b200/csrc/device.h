@@ -98,6 +98,14 @@ void launch_to_aos_mixed(const StepArgs& a, int precision, const void* fin, cons
                          bool gather, const int* st2ref, double* aos, void* stream);
 void launch_from_aos_mixed(const double* aos, const int* st2ref, int n, int64_t np, int precision, void* out,
                            float inv_scale, void* stream);
+// Conserved sums (density, momentum x/y/z) over n sites in FP64, deterministic:
+// one partial per block of kSumSitesPerBlock sites in `scratch` (4 doubles per
+// block), then the partials in block order into `out` (4 doubles, device).
+constexpr int kSumThreads = 256;
+constexpr int kSumSitesPerBlock = 2048;
+int moment_sum_blocks(int64_t n);
+void launch_moment_sums(const double* f, int64_t dir_stride, int64_t site_stride, int64_t n, double* scratch,
+                        double* out, void* stream);
 // AoS reference order <-> SoA storage order.
 void launch_soa_to_aos_f64(const double* soa, int64_t np, const int* st2ref, int n, double* aos, void* stream);
 void launch_aos_to_soa_f64(const double* aos, const int* st2ref, int n, double* soa, int64_t np, void* stream);

@@ -536,6 +536,61 @@ void launch1(const StepArgs& a, int wall, bool gather, bool macro, int which, in
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Conserved sums: total density and momentum over the sites, FP64, in a fixed
+// order (deterministic): pass 1 writes one partial per block into scratch,
+// pass 2 adds the partials in block order.
+// f[i*dir_stride + s*site_stride] is distribution i of site s.
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kSumThreads) k_moment_partial(const double* f, int64_t dir_stride, int64_t site_stride,
+                                                                int64_t n, double* partial) {
+  __shared__ double red[4][kSumThreads];
+  const int64_t base = (int64_t)blockIdx.x * kSumSitesPerBlock;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int k = threadIdx.x; k < kSumSitesPerBlock; k += kSumThreads) {
+    const int64_t s = base + k;
+    if (s >= n) break;
+    double fi[Q];
+#pragma unroll
+    for (int i = 0; i < Q; i++) fi[i] = f[(int64_t)i * dir_stride + s * site_stride];
+    double r, mx, my, mz;
+    moments(fi, r, mx, my, mz);
+    acc[0] += r;
+    acc[1] += mx;
+    acc[2] += my;
+    acc[3] += mz;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) red[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int w = kSumThreads / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+#pragma unroll
+      for (int c = 0; c < 4; c++) red[c][threadIdx.x] = red[c][threadIdx.x] + red[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) partial[4 * (int64_t)blockIdx.x + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void k_moment_final(const double* partial, int nblocks, double* out) {
+  const int c = threadIdx.x;
+  if (c >= 4) return;
+  double acc = 0.0;
+  for (int b = 0; b < nblocks; b++) acc = acc + partial[4 * (int64_t)b + c];
+  out[c] = acc;
+}
+
+int moment_sum_blocks(int64_t n) { return (int)((n + kSumSitesPerBlock - 1) / kSumSitesPerBlock); }
+
+void launch_moment_sums(const double* f, int64_t dir_stride, int64_t site_stride, int64_t n, double* scratch,
+                        double* out, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = moment_sum_blocks(n);
+  if (nb > 0) k_moment_partial<<<nb, kSumThreads, 0, st>>>(f, dir_stride, site_stride, n, scratch);
+  k_moment_final<<<1, 32, 0, st>>>(scratch, nb, out);
+}
+
 void launch_step_f64(const StepArgs& a, int kernel, int wall, bool gather, bool macro, int which, int bulk_block,
                      int general_block, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;

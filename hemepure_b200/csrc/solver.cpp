@@ -547,6 +547,33 @@ void Solver::get_macro(double* rho, double* u, double* wss) {
   }
 }
 
+void Solver::moment_sums(double out[4]) {
+  const int nb = moment_sum_blocks(L_.n);
+  if (sum_scratch_.bytes < (size_t)std::max(1, nb) * 4 * sizeof(double)) {
+    sum_scratch_.alloc((size_t)std::max(1, nb) * 4 * sizeof(double));
+    sum_out_.alloc(4 * sizeof(double));
+  }
+  DeviceBuffer tmp;
+  const double* f;
+  int64_t dir_stride, site_stride;
+  if (mixed()) {
+    tmp.alloc((size_t)L_.n * Q * sizeof(double));
+    to_aos(false, tmp.as<double>());
+    f = tmp.as<double>();
+    dir_stride = 1;
+    site_stride = Q;
+  } else {
+    materialise();
+    f = f_[cur_].as<double>();
+    dir_stride = L_.np;
+    site_stride = 1;
+  }
+  launch_moment_sums(f, dir_stride, site_stride, L_.n, sum_scratch_.as<double>(), sum_out_.as<double>(), stream_);
+  check(cudaGetLastError(), "moment sums launch");
+  check(cudaMemcpyAsync(out, sum_out_.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, stream_), "sums download");
+  check(cudaStreamSynchronize(stream_), "moment_sums");
+}
+
 void Solver::get_wk3(int group, int index, double st[4]) {
   const int idx = group * 16 + index;
   for (size_t k = 0; k < L_.couplings.size(); k++) {

@@ -39,6 +39,8 @@ class Solver {
   // `n` steps with CUDA events around each launch: ms[0] plain bulk kernel,
   // ms[1] general kernel, ms[2] Windkessel kernel (summed over the steps).
   int profile(int64_t n, double ms[3]);
+  // Total density and momentum of the distributions entering the next step.
+  void moment_sums(double out[4]);
 
   void get_fs(double* f);
   void set_fs(const double* f);
@@ -96,6 +98,7 @@ class Solver {
   DeviceBuffer g_site_, g_wall_, g_iolet_, g_src_, g_q_, g_nrm_, g_io_, g_cpl_, g_xyz_;
   DeviceBuffer vtau_, iolets_, dens_, cpl_buf_, wk3_, status_;
   DeviceBuffer rho_, u_, wss_;
+  DeviceBuffer sum_scratch_, sum_out_;
   int dens_rows_ = 0;
   int row_ = 0;                   // row of the density table used by the current step
   std::vector<double> host_rows_;

@@ -38,7 +38,7 @@ EXPORTS = [
     "hb_get_macro", "hb_get_wk3", "hb_get_tables", "hb_write_xtr", "hb_read_checkpoint",
     "hb_last_step_timing", "hb_device_bytes", "hb_read_case", "hb_geometry_open", "hb_geometry_site_count",
     "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_close", "hb_profile_steps",
-    "hb_set_time_step",
+    "hb_set_time_step", "hb_moment_sums",
 ]
 
 
@@ -120,6 +120,7 @@ def library() -> C.CDLL:
     L.hb_geometry_close.argtypes = [P]
     L.hb_profile_steps.argtypes = [P, I64, P]
     L.hb_set_time_step.argtypes = [P, U64]
+    L.hb_moment_sums.argtypes = [P, P]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name != "hb_default_options":
@@ -259,6 +260,12 @@ class LBM:
         w = np.empty(self.n)
         self._check(library().hb_get_macro(self._h, _p(rho), _p(u), _p(w)))
         return rho, u, w
+
+    def moment_sums(self) -> np.ndarray:
+        """(total density, total momentum x, y, z) of the current distributions, FP64."""
+        a = np.empty(4)
+        self._check(library().hb_moment_sums(self._h, _p(a)))
+        return a
 
     def GetWK3(self, group: int, index: int) -> np.ndarray:
         a = np.empty(4)

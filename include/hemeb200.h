@@ -161,6 +161,10 @@ int hb_set_fs(hb_handle* h, const double* f);
  * [n*3], wall-shear-stress magnitude [n] (NO_VALUE = DBL_MAX off the wall).
  * Any pointer may be NULL. */
 int hb_get_macro(hb_handle* h, double* density, double* velocity, double* wss);
+/* Total density and momentum (x, y, z) of the distributions entering the next
+ * step, summed in FP64 in a fixed order: the per-step mass and flux balance
+ * the reference's monitoring computes on the host (src/lb/IncompressibilityChecker.hpp). */
+int hb_moment_sums(hb_handle* h, double sums[4]);
 /* Windkessel state of iolet `index` of `group` (0 inlets, 1 outlets):
  * density, densityNew, flowRate, flowRateOld (InOutLetWK3 members). */
 int hb_get_wk3(hb_handle* h, int group, int index, double state[4]);

@@ -101,3 +101,19 @@ def test_instability_is_reported(case_dir):
     gpu.SetFs(f)
     with pytest.raises(lbm.Unstable):
         gpu.step(2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_moment_sums_match_distributions(case_dir, precision):
+    """hb_moment_sums equals the density and momentum summed from GetFOld on the host."""
+    xml, gmy, info, kernel, wall, _ = make_small_case(case_dir, "pipe_bfl")
+    g = lbm.LBM(xml, kernel=kernel, wall=wall, precision=precision)
+    g.step(40)
+    sums = g.moment_sums()
+    f = g.GetFOld()
+    cx = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0], float)
+    cy = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1], float)
+    cz = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1], float)
+    ref = np.array([f.sum(), (f * cx).sum(), (f * cy).sum(), (f * cz).sum()])
+    assert abs(sums[0] - ref[0]) <= 1e-12 * abs(ref[0])
+    assert np.max(np.abs(sums[1:] - ref[1:])) <= 1e-12 * abs(ref[0])
