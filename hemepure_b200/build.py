@@ -23,6 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = {
     "kernels_f64.cu": ["-fmad=false"],
     "kernels_mixed.cu": [],
+    "noalloc.cu": [],
 }
 CPP_SOURCES = ["xml.cpp", "config.cpp", "layout.cpp", "solver.cpp", "extraction.cpp", "capi.cpp"]
 HEADERS = ["hb_common.h", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h"]

@@ -38,7 +38,7 @@ EXPORTS = [
     "hb_get_macro", "hb_get_wk3", "hb_get_tables", "hb_write_xtr", "hb_read_checkpoint",
     "hb_last_step_timing", "hb_device_bytes", "hb_read_case", "hb_geometry_open", "hb_geometry_site_count",
     "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_close", "hb_profile_steps",
-    "hb_set_time_step", "hb_moment_sums",
+    "hb_set_time_step", "hb_moment_sums", "hb_moment_sums_noalloc",
 ]
 
 
@@ -121,6 +121,7 @@ def library() -> C.CDLL:
     L.hb_profile_steps.argtypes = [P, I64, P]
     L.hb_set_time_step.argtypes = [P, U64]
     L.hb_moment_sums.argtypes = [P, P]
+    L.hb_moment_sums_noalloc.argtypes = [P, I64, I64, I64, P, P]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name != "hb_default_options":

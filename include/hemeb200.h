@@ -205,6 +205,23 @@ int hb_geometry_tables(const hb_geometry* g, int64_t* neighbours, uint32_t* wall
 int hb_geometry_layout(const hb_geometry* g, const hb_params* params, int wall, int64_t stats[4]);
 int hb_geometry_close(hb_geometry* g);
 
+/* ---- without device allocation --------------------------------------------------- */
+
+/* Total density and momentum (x, y, z) of n_sites sites, like hb_moment_sums but
+ * on device buffers the caller owns, for callers whose device memory is all
+ * committed elsewhere (their own pool or a fixed HBM budget) and who must not
+ * have the library allocate.  No reference counterpart: the reference sums on
+ * the host.  Distribution i of site s is f[i*dir_stride + s*site_stride] (FP64,
+ * device); the four sums go to `sums` (device) on `stream` (a cudaStream_t, or
+ * NULL).  Nothing is allocated: the scratch is a fixed 256 KiB array in the
+ * library, so one call takes at most 16,777,216 sites (more returns HB_ERR_ARG).
+ * The first call on a device looks up that array's device address (once per
+ * device); make it before any stream capture.  Calls share the array, so two
+ * calls whose kernels overlap on one GPU race; the result is ready when
+ * `stream` is synchronised.  Errors: hb_last_error(NULL, ...). */
+int hb_moment_sums_noalloc(const double* f, int64_t dir_stride, int64_t site_stride, int64_t n_sites, double* sums,
+                           void* stream);
+
 /* ---- measurement helpers ----------------------------------------------------- */
 
 /* Device-time of the last hb_step call's kernels in milliseconds (CUDA events),
