@@ -24,9 +24,10 @@ CU_SOURCES = {
     "kernels_f64.cu": ["-fmad=false"],
     "kernels_mixed.cu": [],
     "noalloc.cu": [],
+    "kernels_batch.cu": [],
 }
-CPP_SOURCES = ["xml.cpp", "config.cpp", "layout.cpp", "solver.cpp", "extraction.cpp", "capi.cpp"]
-HEADERS = ["hb_common.h", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h"]
+CPP_SOURCES = ["xml.cpp", "config.cpp", "layout.cpp", "solver.cpp", "extraction.cpp", "batch.cpp", "capi.cpp"]
+HEADERS = ["hb_common.h", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h", "mixed_site.cuh", "batch.h", "batch_dev.h"]
 
 
 def _deps_mtime() -> float:

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "../../include/hemeb200.h"
+#include "batch.h"
 #include "config.h"
 #include "extraction.h"
 #include "solver.h"
@@ -16,6 +17,10 @@ struct hb_handle {
 
 struct hb_geometry {
   hb::LatticeTables tables;
+};
+
+struct hb_batch {
+  std::unique_ptr<hb::Batch> batch;
 };
 
 namespace {
@@ -269,6 +274,127 @@ int hb_read_checkpoint(hb_handle* h, const char* path, uint64_t step) {
     hb::read_checkpoint(*h->solver, path, step);
     return HB_OK;
   });
+}
+
+namespace {
+
+hb::LatticeTables tables_from_desc(const hb_lattice_desc* lat) {
+  hb::LatticeTables t;
+  const int64_t n = lat->n_sites;
+  t.n = n;
+  for (int d = 0; d < 3; d++) t.dims[d] = lat->dims[d];
+  t.coords.assign(lat->coords, lat->coords + 3 * n);
+  t.wall.assign(lat->wall_mask, lat->wall_mask + n);
+  t.iolet.assign(lat->iolet_mask, lat->iolet_mask + n);
+  t.stype.assign(lat->site_type, lat->site_type + n);
+  t.iolet_id.assign(lat->iolet_id, lat->iolet_id + n);
+  if (lat->wall_distance) t.q.assign(lat->wall_distance, lat->wall_distance + 18 * n);
+  if (lat->wall_normal) t.normal.assign(lat->wall_normal, lat->wall_normal + 3 * n);
+  else t.normal.assign(3 * n, 0.0);
+  for (int64_t i = 0; i < n; i++) t.type_counts[t.collision_type(i)]++;
+  if (lat->neighbours) t.nbr.assign(lat->neighbours, lat->neighbours + 19 * n);
+  else hb::build_neighbours(t);
+  return t;
+}
+
+}  // namespace
+
+int hb_batch_bytes(int64_t site_capacity, int64_t general_capacity, int max_lattices, int precision, int64_t* bytes) {
+  if (!bytes) return HB_ERR_ARG;
+  *bytes = hb::Batch::bytes_for(site_capacity, general_capacity, max_lattices, precision);
+  return HB_OK;
+}
+
+int hb_batch_create(int64_t site_capacity, int64_t general_capacity, int max_lattices, int precision, int device,
+                    hb_batch** out) {
+  if (!out) return HB_ERR_ARG;
+  *out = nullptr;
+  return guard(nullptr, [&] {
+    auto b = std::make_unique<hb_batch>();
+    b->batch = std::make_unique<hb::Batch>(site_capacity, general_capacity, max_lattices, precision, device);
+    *out = b.release();
+    return HB_OK;
+  });
+}
+
+int hb_batch_destroy(hb_batch* b) {
+  if (!b) return HB_ERR_ARG;
+  delete b;
+  return HB_OK;
+}
+
+int hb_batch_add_xml(hb_batch* b, const char* xml_path, int kernel, int wall, uint64_t steps, int* slot) {
+  if (!b || !xml_path || !slot) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    hb::CaseConfig c = hb::read_case(xml_path, kernel);
+    *slot = b->batch->add(hb::read_gmy(c.gmy_path), c.params, kernel, wall, steps);
+    return HB_OK;
+  });
+}
+
+int hb_batch_add(hb_batch* b, const hb_lattice_desc* lat, const hb_params* params, int kernel, int wall, uint64_t steps,
+                 int* slot) {
+  if (!b || !lat || !params || !slot || lat->n_sites <= 0 || !lat->coords || !lat->wall_mask || !lat->iolet_mask ||
+      !lat->site_type || !lat->iolet_id)
+    return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    *slot = b->batch->add(tables_from_desc(lat), *params, kernel, wall, steps);
+    return HB_OK;
+  });
+}
+
+int hb_batch_remove(hb_batch* b, int slot) {
+  if (!b) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    b->batch->remove(slot);
+    return HB_OK;
+  });
+}
+
+int hb_batch_run(hb_batch* b, int k, int* finished, int max_finished, int* n_finished) {
+  if (!b || k < 0) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    std::vector<int> done = b->batch->run(k);
+    int m = 0;
+    for (int s : done)
+      if (finished && m < max_finished) finished[m++] = s;
+    if (n_finished) *n_finished = finished ? m : (int)done.size();
+    return HB_OK;
+  });
+}
+
+int hb_batch_get_macro(hb_batch* b, int slot, double* density, double* velocity, double* wss) {
+  if (!b) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    b->batch->get_macro(slot, density, velocity, wss);
+    return HB_OK;
+  });
+}
+
+int hb_batch_member_info(hb_batch* b, int slot, int64_t* sites, uint64_t* time_step, int* status) {
+  if (!b) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    if (sites) *sites = b->batch->member_sites(slot);
+    if (time_step) *time_step = b->batch->time_step(slot);
+    if (status) *status = b->batch->status(slot);
+    return HB_OK;
+  });
+}
+
+int hb_batch_set_tuning(hb_batch* b, int sites_per_thread, int block) {
+  if (!b) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    b->batch->set_tuning(sites_per_thread, block);
+    return HB_OK;
+  });
+}
+
+int hb_batch_stats(const hb_batch* b, double* last_block_ms, int64_t* active_sites, int64_t* device_bytes) {
+  if (!b) return HB_ERR_ARG;
+  if (last_block_ms) *last_block_ms = b->batch->last_ms();
+  if (active_sites) *active_sites = b->batch->active_sites();
+  if (device_bytes) *device_bytes = b->batch->device_bytes();
+  return HB_OK;
 }
 
 int hb_read_case(const char* xml_path, int kernel, hb_params* params, char* gmy_path, size_t gmy_path_len) {

@@ -39,6 +39,8 @@ EXPORTS = [
     "hb_last_step_timing", "hb_device_bytes", "hb_read_case", "hb_geometry_open", "hb_geometry_site_count",
     "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_close", "hb_profile_steps",
     "hb_set_time_step", "hb_moment_sums", "hb_moment_sums_noalloc",
+    "hb_batch_bytes", "hb_batch_create", "hb_batch_destroy", "hb_batch_add_xml", "hb_batch_add", "hb_batch_remove",
+    "hb_batch_run", "hb_batch_get_macro", "hb_batch_member_info", "hb_batch_set_tuning", "hb_batch_stats",
 ]
 
 
@@ -122,6 +124,17 @@ def library() -> C.CDLL:
     L.hb_set_time_step.argtypes = [P, U64]
     L.hb_moment_sums.argtypes = [P, P]
     L.hb_moment_sums_noalloc.argtypes = [P, I64, I64, I64, P, P]
+    L.hb_batch_bytes.argtypes = [I64, I64, I, I, P]
+    L.hb_batch_create.argtypes = [I64, I64, I, I, I, C.POINTER(P)]
+    L.hb_batch_destroy.argtypes = [P]
+    L.hb_batch_add_xml.argtypes = [P, C.c_char_p, I, I, U64, P]
+    L.hb_batch_add.argtypes = [P, P, P, I, I, U64, P]
+    L.hb_batch_remove.argtypes = [P, I]
+    L.hb_batch_run.argtypes = [P, I, P, I, P]
+    L.hb_batch_get_macro.argtypes = [P, I, P, P, P]
+    L.hb_batch_member_info.argtypes = [P, I, P, P, P]
+    L.hb_batch_set_tuning.argtypes = [P, I, I]
+    L.hb_batch_stats.argtypes = [P, P, P, P]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name != "hb_default_options":
@@ -364,6 +377,76 @@ class Geometry:
         if getattr(self, "_g", None) and self._g.value:
             library().hb_geometry_close(self._g)
             self._g = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many lattices resident on one GPU, stepped together (the batched form)."""
+
+    def __init__(self, site_capacity: int, general_capacity: int, max_lattices: int = 64,
+                 precision: str = "fp32", device: int = 0):
+        self._b = C.c_void_p()
+        rc = library().hb_batch_create(int(site_capacity), int(general_capacity), int(max_lattices),
+                                       PRECISIONS[precision], int(device), C.byref(self._b))
+        if rc != HB_OK:
+            raise HemeLBError(rc, last_create_error())
+        self.max_lattices = int(max_lattices)
+
+    @staticmethod
+    def bytes_for(site_capacity: int, general_capacity: int, max_lattices: int = 64, precision: str = "fp32") -> int:
+        b = C.c_int64()
+        library().hb_batch_bytes(int(site_capacity), int(general_capacity), int(max_lattices), PRECISIONS[precision],
+                                 C.byref(b))
+        return int(b.value)
+
+    def _check(self, rc):
+        if rc != HB_OK:
+            raise HemeLBError(rc, last_create_error())
+
+    def add_xml(self, xml_path: str, kernel: str = "LBGK", wall: str = "SBB", steps: int = 1000) -> int:
+        slot = C.c_int()
+        self._check(library().hb_batch_add_xml(self._b, os.fspath(xml_path).encode(), KERNELS[kernel], WALLS[wall],
+                                               int(steps), C.byref(slot)))
+        return int(slot.value)
+
+    def remove(self, slot: int) -> None:
+        self._check(library().hb_batch_remove(self._b, int(slot)))
+
+    def run(self, k: int):
+        """Run k steps; returns the slots that finished in this block."""
+        buf = (C.c_int * self.max_lattices)()
+        n = C.c_int()
+        self._check(library().hb_batch_run(self._b, int(k), buf, self.max_lattices, C.byref(n)))
+        return [int(buf[i]) for i in range(n.value)]
+
+    def macro(self, slot: int):
+        n, _, _ = self.info(slot)
+        rho, u, w = np.empty(n), np.empty((n, 3)), np.empty(n)
+        self._check(library().hb_batch_get_macro(self._b, int(slot), _p(rho), _p(u), _p(w)))
+        return rho, u, w
+
+    def info(self, slot: int):
+        n, t, st = C.c_int64(), C.c_uint64(), C.c_int()
+        self._check(library().hb_batch_member_info(self._b, int(slot), C.byref(n), C.byref(t), C.byref(st)))
+        return int(n.value), int(t.value), int(st.value)
+
+    def set_tuning(self, sites_per_thread: int, block: int) -> None:
+        self._check(library().hb_batch_set_tuning(self._b, int(sites_per_thread), int(block)))
+
+    def stats(self):
+        ms, act, by = C.c_double(), C.c_int64(), C.c_int64()
+        library().hb_batch_stats(self._b, C.byref(ms), C.byref(act), C.byref(by))
+        return float(ms.value), int(act.value), int(by.value)
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            library().hb_batch_destroy(self._b)
+            self._b = C.c_void_p()
 
     def __del__(self):
         try:

@@ -186,6 +186,39 @@ int hb_write_xtr(hb_handle* h, const char* path, const char* fields, const char*
  * (LocalDistributionInput::LoadDistribution). */
 int hb_read_checkpoint(hb_handle* h, const char* path, uint64_t step);
 
+/* ---- batched form: many lattices of uneven size on one GPU ------------------------ */
+
+/* The batched form keeps many independent lattices resident in one device arena
+ * (shifted FP32 or FP16 storage) and steps them together: per step one
+ * persistent kernel over every member's plain bulk sites and one over every
+ * member's boundary sites, with per-lattice relaxation times, iolets and time
+ * counters in device memory, the steps of a block captured once in a CUDA graph.
+ * Members are admitted and retired between blocks without moving the others.
+ * Supported per member: LBGK or TRT, bounce-back or BFL walls, cosine pressure
+ * and parabolic velocity iolets.  Capacities: sites (rounded to 64 per member),
+ * boundary records, member slots. */
+typedef struct hb_batch hb_batch;
+int hb_batch_bytes(int64_t site_capacity, int64_t general_capacity, int max_lattices, int precision, int64_t* bytes);
+int hb_batch_create(int64_t site_capacity, int64_t general_capacity, int max_lattices, int precision, int device,
+                    hb_batch** out);
+int hb_batch_destroy(hb_batch* b);
+/* Admit a lattice for `steps` time steps; returns its slot.  HB_ERR_OOM when it does not fit. */
+int hb_batch_add_xml(hb_batch* b, const char* xml_path, int kernel, int wall, uint64_t steps, int* slot);
+int hb_batch_add(hb_batch* b, const hb_lattice_desc* lat, const hb_params* params, int kernel, int wall, uint64_t steps,
+                 int* slot);
+int hb_batch_remove(hb_batch* b, int slot);
+/* Run a block of k steps; the slots that reached their step count are written
+ * to finished[0 .. *n_finished) (at most max_finished). */
+int hb_batch_run(hb_batch* b, int k, int* finished, int max_finished, int* n_finished);
+/* Density [n], velocity [n*3], wall shear stress [n] of a finished member's last step, reference order. */
+int hb_batch_get_macro(hb_batch* b, int slot, double* density, double* velocity, double* wss);
+/* Member sites, time step reached, status bits (1 unstable, 2 iolet radius). */
+int hb_batch_member_info(hb_batch* b, int slot, int64_t* sites, uint64_t* time_step, int* status);
+/* Sites per thread (1, 2) and threads per block (128, 256, 512) of the bulk kernel. */
+int hb_batch_set_tuning(hb_batch* b, int sites_per_thread, int block);
+/* Device time of the last block in ms, active sites, device bytes held. */
+int hb_batch_stats(const hb_batch* b, double* last_block_ms, int64_t* active_sites, int64_t* device_bytes);
+
 /* ---- host-only readers (no GPU needed) ------------------------------------------ */
 
 /* SimConfig::DoIO for the collide-and-stream path: lattice-unit parameters and
