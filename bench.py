@@ -134,6 +134,33 @@ def cpu_baseline(xml: str, kernel: str, wall: str, n_sites: int, budget_s: float
                       f"({n_sites * steps} site updates, {dt:.1f} s, {threads} threads, status {rc})"}
 
 
+def serving_leg(n_requests: int, device: int, case_root: str):
+    """Continuous batching of a seeded stream of vessel solves (FP32-shifted batched
+    form): Poisson arrivals at 80% of the measured capacity under a 150 GB budget."""
+    from hemepure_b200 import serving
+    t0 = time.perf_counter()
+    reqs = serving.generate_requests(n_requests, os.path.join(case_root, "serving"), seed=2024)
+    gen_s = time.perf_counter() - t0
+    tuning = serving.autotune(reqs[:4], tolerance=1e-4, device=device)
+    works = np.array([r.sites * r.steps for r in reqs], dtype=np.float64)
+    rate = 0.8 * tuning.mlups * 1e6 / float(works.mean())
+    serving.poisson_arrivals(reqs, rate)
+    srv = serving.Server(150 * 10 ** 9, device=device, tuning=tuning, block_steps=200)
+    srv.run(reqs)
+    rep = srv.report()
+    sample = reqs[:8]
+    seq = serving.solve_sequential_fp64(sample, device=device)
+    rep.update({"stream": f"{n_requests} seeded vessels (pipe / Y-bifurcation / 50-75% stenosis), r~U[6,32], "
+                          f"L~U[10,40]r, LBGK/TRT tau~U[0.51,1], pressure or parabolic inlet Re<=300, "
+                          f"1000-20000 steps", "storage": tuning.precision,
+                "tuning": {"sites_per_thread": tuning.sites_per_thread, "block": tuning.block,
+                           "probe_MLUPS": tuning.mlups, "table": tuning.table},
+                "arrival_rate_per_s": rate, "geometry_generation_s": gen_s,
+                "fp64_one_at_a_time_MLUPS": seq["MLUPS"], "fp64_sample_requests": seq["requests"],
+                "speedup_vs_fp64_one_at_a_time": rep["aggregate_MLUPS"] / seq["MLUPS"]})
+    return rep
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -143,6 +170,8 @@ def main():
     ap.add_argument("--workload", default="pipe_r40", choices=sorted(WORKLOADS))
     ap.add_argument("--case-dir", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=128,
+                    help="requests in the serving leg (0 skips it; 512 is the full stream)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -273,6 +302,13 @@ def main():
         except Exception as e:  # report, do not hide
             forms[prec] = {"error": str(e)}
 
+    serving_rep = None
+    if world == 1 and args.serving_requests > 0:
+        try:
+            serving_rep = serving_leg(args.serving_requests, local, case_root)
+        except Exception as e:  # report, do not hide
+            serving_rep = {"error": repr(e)}
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(xml, kernel, wall, n_sites)
@@ -282,6 +318,7 @@ def main():
                 "warmup": warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
                 "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "clocks": clocks, "forms": forms,
+                "serving": serving_rep,
                 "gpu_launches": int(launches), "wall_s": wall_s}
         print(json.dumps(line), flush=True)
     sim.close()

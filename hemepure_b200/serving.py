@@ -1,0 +1,269 @@
+"""Serving loop over the batched form: continuous batching of solve requests.
+
+Requests (geometry, relaxation time, inlet profile, step count) arrive over
+time; the server admits each as soon as the batch has a free slot and room in
+its HBM budget, keeps every admitted lattice resident on the device, steps all
+of them together in CUDA-graph blocks, and retires each at its step count with
+its extractions (density, velocity, wall shear stress of the last step).
+Latency is arrival to retirement; throughput is site updates per second over
+the run.
+"""
+
+from __future__ import annotations
+
+import math
+import os
+import tempfile
+import time
+from collections import deque
+from concurrent.futures import ProcessPoolExecutor
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import lbm, vessels
+
+
+@dataclass
+class Request:
+    rid: int
+    xml: str
+    kernel: str
+    wall: str
+    steps: int
+    sites: int
+    arrival: float = 0.0
+    shape: str = ""
+    # filled by the server
+    admitted: Optional[float] = None
+    finished: Optional[float] = None
+    result: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
+    status: int = 0
+
+    @property
+    def latency(self) -> Optional[float]:
+        return None if self.finished is None else self.finished - self.arrival
+
+
+# ---------------------------------------------------------------------------
+# The request mix: seeded random vessels
+# ---------------------------------------------------------------------------
+
+def _make_request(args) -> Tuple[int, str, str, str, int, int, str]:
+    (rid, out_dir, seed, r_range, l_range, step_range, re_max) = args
+    rng = np.random.default_rng([seed, rid])
+    shape = ["pipe", "bifurcation", "stenosis"][int(rng.integers(0, 3))]
+    r = float(rng.uniform(*r_range))
+    length = float(rng.uniform(*l_range)) * r
+    kernel = "LBGK" if rng.random() < 0.5 else "TRT"
+    tau = float(rng.uniform(0.51, 1.0))
+    nu = (tau - 0.5) / 3.0
+    # velocity at Re <= re_max, capped for the lattice's Mach limit
+    u = min(re_max * nu / (2.0 * r), 0.05) * float(rng.uniform(0.5, 1.0))
+    steps = int(rng.integers(step_range[0], step_range[1] + 1))
+    ri = max(3, int(round(r)))
+    li = max(8, int(round(length)))
+    if shape == "pipe":
+        v = vessels.Pipe(ri, li)
+    elif shape == "stenosis":
+        sev = float(rng.uniform(0.5, 0.75))          # area reduction
+        rmin = max(2.0, ri * math.sqrt(1.0 - sev))
+        v = vessels.Stenosis(ri, li, rmin, max(4.0, 2.0 * ri))
+    else:
+        rd = max(3, int(round(ri * 0.8)))
+        v = vessels.YBifurcation(ri, li // 2, rd, li // 2, 35.0)
+    d = os.path.join(out_dir, f"req{rid:05d}")
+    os.makedirs(d, exist_ok=True)
+    gmy = os.path.join(d, "geom.gmy")
+    xml = os.path.join(d, "case.xml")
+    info = vessels.voxelise(v, gmy)
+    units = vessels.CaseUnits(tau=tau)
+    n_out = len([io for io in v.iolets if io.kind == "outlet"])
+    if rng.random() < 0.5:
+        inlet = [vessels.VelocityBC(u)]
+        warm = int(min(1000, steps // 4))
+    else:
+        # pressure drop that drives about u through a Poiseuille tube of this size
+        drho = 3.0 * 8.0 * nu * u * length / (r * r) / 2.0
+        inlet = [vessels.PressureBC(1.0 + drho)]
+        warm = 0
+    outlets = [vessels.PressureBC(1.0)] * n_out
+    vessels.write_case_xml(xml, "geom.gmy", v, units, max(1, steps - warm), inlet, outlets, warmup=warm,
+                           relaxation_parameter=3.0 / 16.0 if kernel == "TRT" else None)
+    wall = "BFL" if rng.random() < 0.5 else "SBB"
+    return rid, xml, kernel, wall, steps, info.fluid_sites, shape
+
+
+def generate_requests(n: int, out_dir: Optional[str] = None, seed: int = 2024,
+                      radius: Tuple[float, float] = (6.0, 32.0), length_radii: Tuple[float, float] = (10.0, 40.0),
+                      steps: Tuple[int, int] = (1000, 20000), re_max: float = 300.0,
+                      workers: int = 0) -> List[Request]:
+    """Seeded random vessels: straight pipe, Y-bifurcation at +-35 degrees, or
+    50-75 % cosine stenosis with equal probability; radius U[r0, r1], length
+    U[l0, l1] radii; LBGK or TRT with tau ~ U[0.51, 1.0]; pressure or parabolic
+    velocity inlet at Re <= re_max; step count U[s0, s1]."""
+    out_dir = out_dir or tempfile.mkdtemp(prefix="hemeb200_requests_")
+    jobs = [(i, out_dir, seed, radius, length_radii, steps, re_max) for i in range(n)]
+    workers = workers or min(16, os.cpu_count() or 1)
+    if workers > 1 and n > 1:
+        import multiprocessing as mp
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            made = list(ex.map(_make_request, jobs))
+    else:
+        made = [_make_request(j) for j in jobs]
+    return [Request(rid=m[0], xml=m[1], kernel=m[2], wall=m[3], steps=m[4], sites=m[5], shape=m[6]) for m in made]
+
+
+def poisson_arrivals(requests: Sequence[Request], rate_per_s: float, seed: int = 7) -> None:
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    for r in requests:
+        t += float(rng.exponential(1.0 / rate_per_s))
+        r.arrival = t
+
+
+# ---------------------------------------------------------------------------
+# Autotuner
+# ---------------------------------------------------------------------------
+
+@dataclass
+class Tuning:
+    sites_per_thread: int
+    block: int
+    precision: str
+    mlups: float
+    table: Dict[str, float] = field(default_factory=dict)
+
+
+def autotune(probe: Sequence[Request], tolerance: float = 1e-4, device: int = 0, block_steps: int = 64,
+             site_capacity: Optional[int] = None) -> Tuning:
+    """Pick sites per thread, threads per block and storage precision.
+
+    Precision: FP16 storage is only eligible when the tolerance allows its error
+    (about 1e-3 relative in velocity against FP64); otherwise FP32.  The launch
+    shape is timed on a probe batch holding the given requests."""
+    precisions = ["fp32"] + (["fp16"] if tolerance >= 5e-3 else [])
+    total = sum(r.sites for r in probe)
+    cap = site_capacity or int(total * 1.1) + 64 * len(probe) + 1024
+    best = None
+    table = {}
+    for prec in precisions:
+        b = lbm.Batch(cap, cap, max(8, len(probe)), precision=prec, device=device)
+        for r in probe:
+            b.add_xml(r.xml, r.kernel, r.wall, 10 ** 9)
+        for spt in (1, 2):
+            for block in (128, 256, 512):
+                b.set_tuning(spt, block)
+                b.run(block_steps)          # capture + warm
+                b.run(block_steps)
+                ms, act, _ = b.stats()
+                mlups = act * block_steps / (ms * 1e-3) / 1e6
+                table[f"{prec}/spt{spt}/b{block}"] = mlups
+                if best is None or mlups > best.mlups:
+                    best = Tuning(spt, block, prec, mlups)
+        b.close()
+    best.table = table
+    return best
+
+
+# ---------------------------------------------------------------------------
+# Server
+# ---------------------------------------------------------------------------
+
+class Server:
+    """Continuous batching of solve requests on one GPU under an HBM budget."""
+
+    def __init__(self, budget_bytes: int, device: int = 0, tuning: Optional[Tuning] = None, block_steps: int = 100,
+                 max_lattices: int = 256, general_fraction: float = 0.6):
+        precision = tuning.precision if tuning else "fp32"
+        # Largest site capacity whose arena fits the budget.
+        lo, hi = 1024, 1 << 31
+        while lo < hi:
+            mid = (lo + hi + 1) // 2
+            need = lbm.Batch.bytes_for(mid, int(mid * general_fraction), max_lattices, precision)
+            if need <= budget_bytes:
+                lo = mid
+            else:
+                hi = mid - 1
+        self.site_capacity = lo
+        self.batch = lbm.Batch(lo, int(lo * general_fraction), max_lattices, precision=precision, device=device)
+        if tuning:
+            self.batch.set_tuning(tuning.sites_per_thread, tuning.block)
+        self.block_steps = block_steps
+        self.queue: deque = deque()
+        self.running: Dict[int, Request] = {}
+        self.completed: List[Request] = []
+        self.site_updates = 0
+        self.device_ms = 0.0
+
+    def submit(self, r: Request) -> None:
+        self.queue.append(r)
+
+    def _admit(self, now: float) -> None:
+        while self.queue and self.queue[0].arrival <= now:
+            r = self.queue[0]
+            try:
+                slot = self.batch.add_xml(r.xml, r.kernel, r.wall, r.steps)
+            except lbm.HemeLBError as e:
+                if e.code == -5:      # no room yet: wait for a retirement (FIFO)
+                    if not self.running:
+                        raise RuntimeError(f"request {r.rid} ({r.sites} sites) exceeds the whole budget") from e
+                    return
+                raise
+            r.admitted = now
+            self.running[slot] = r
+            self.queue.popleft()
+
+    def run(self, requests: Sequence[Request], keep_results: bool = False, clock=time.perf_counter) -> None:
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        t0 = clock()
+        while pending or self.queue or self.running:
+            now = clock() - t0
+            while pending and pending[0].arrival <= now:
+                self.submit(pending.popleft())
+            self._admit(now)
+            if not self.running:
+                if pending:
+                    time.sleep(max(0.0, min(0.05, pending[0].arrival - (clock() - t0))))
+                continue
+            active = self.batch.stats()[1]
+            done = self.batch.run(self.block_steps)
+            ms = self.batch.stats()[0]
+            self.device_ms += ms
+            self.site_updates += active * self.block_steps
+            now = clock() - t0
+            for slot in done:
+                r = self.running.pop(slot)
+                n, t, st = self.batch.info(slot)
+                r.status = st
+                res = self.batch.macro(slot)
+                if keep_results:
+                    r.result = res
+                r.finished = now
+                self.batch.remove(slot)
+                self.completed.append(r)
+        self.wall_s = clock() - t0
+
+    def report(self) -> Dict[str, float]:
+        lat = np.array([r.latency for r in self.completed])
+        work = sum(r.sites * r.steps for r in self.completed)
+        return {"requests": len(self.completed), "p50_latency_s": float(np.percentile(lat, 50)),
+                "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
+                "aggregate_MLUPS": work / self.wall_s / 1e6, "wall_s": self.wall_s,
+                "device_busy_MLUPS": self.site_updates / (self.device_ms * 1e-3) / 1e6 if self.device_ms else 0.0,
+                "site_capacity": self.site_capacity, "failed": int(sum(1 for r in self.completed if r.status))}
+
+
+def solve_sequential_fp64(requests: Sequence[Request], device: int = 0) -> Dict[str, float]:
+    """The same requests one at a time on the FP64 plain path (create, step, extract)."""
+    t0 = time.perf_counter()
+    work = 0
+    for r in requests:
+        sim = lbm.LBM(r.xml, kernel=r.kernel, wall=r.wall, device=device)
+        sim.step(r.steps, macro=True)
+        sim.GetPropertyCache()
+        sim.close()
+        work += r.sites * r.steps
+    dt = time.perf_counter() - t0
+    return {"requests": len(requests), "MLUPS": work / dt / 1e6, "wall_s": dt}
