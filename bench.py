@@ -170,7 +170,7 @@ def main():
     ap.add_argument("--workload", default="pipe_r40", choices=sorted(WORKLOADS))
     ap.add_argument("--case-dir", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--serving-requests", type=int, default=128,
+    ap.add_argument("--serving-requests", type=int, default=64,
                     help="requests in the serving leg (0 skips it; 512 is the full stream)")
     args = ap.parse_args()
 

@@ -146,8 +146,8 @@ Batch::~Batch() {
 }
 
 void Batch::set_tuning(int spt, int bulk_block) {
-  if ((spt != 1 && spt != 2) || (bulk_block != 128 && bulk_block != 256 && bulk_block != 512))
-    throw Error{HB_ERR_ARG, "sites per thread must be 1 or 2 and the block 128, 256 or 512 threads"};
+  if ((spt != 1 && spt != 2) || (bulk_block != 128 && bulk_block != 256))
+    throw Error{HB_ERR_ARG, "sites per thread must be 1 or 2 and the block 128 or 256 threads"};
   spt_ = spt;
   bulk_block_ = bulk_block;
   dirty_ = true;

@@ -153,7 +153,7 @@ def autotune(probe: Sequence[Request], tolerance: float = 1e-4, device: int = 0,
         for r in probe:
             b.add_xml(r.xml, r.kernel, r.wall, 10 ** 9)
         for spt in (1, 2):
-            for block in (128, 256, 512):
+            for block in (128, 256):
                 b.set_tuning(spt, block)
                 b.run(block_steps)          # capture + warm
                 b.run(block_steps)

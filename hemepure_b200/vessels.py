@@ -287,6 +287,8 @@ def voxelise(vessel: Vessel, path: str, block_size: int = 8, chunk_blocks: int =
         gz = (bzs[b0:b1, None] * bs + lz[None, :]).reshape(-1)
         fidx = np.nonzero(fl)[0]
         nf = len(fidx)
+        if nf == 0:
+            continue  # every block of this chunk is solid: empty headers, no bodies
         # Word layout per fluid site: 1 + 26*3 + 1 + 3 = 83 slots, masked.
         words = np.zeros((nf, 83), dtype=np.uint32)
         valid = np.zeros((nf, 83), dtype=bool)

@@ -214,7 +214,7 @@ int hb_batch_run(hb_batch* b, int k, int* finished, int max_finished, int* n_fin
 int hb_batch_get_macro(hb_batch* b, int slot, double* density, double* velocity, double* wss);
 /* Member sites, time step reached, status bits (1 unstable, 2 iolet radius). */
 int hb_batch_member_info(hb_batch* b, int slot, int64_t* sites, uint64_t* time_step, int* status);
-/* Sites per thread (1, 2) and threads per block (128, 256, 512) of the bulk kernel. */
+/* Sites per thread (1, 2) and threads per block (128, 256) of the bulk kernel. */
 int hb_batch_set_tuning(hb_batch* b, int sites_per_thread, int block);
 /* Device time of the last block in ms, active sites, device bytes held. */
 int hb_batch_stats(const hb_batch* b, double* last_block_ms, int64_t* active_sites, int64_t* device_bytes);
