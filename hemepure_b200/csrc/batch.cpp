@@ -80,9 +80,8 @@ Batch::Batch(int64_t site_capacity, int64_t general_capacity, int max_lattices, 
     : device_(device), precision_(precision) {
   if (precision != HB_STORE_FP32 && precision != HB_STORE_FP16)
     throw Error{HB_ERR_UNSUPPORTED, "the batched form stores shifted FP32 or FP16 distributions"};
-  if (site_capacity <= 0 || site_capacity > ((int64_t)1 << 31) - 64 || max_lattices <= 0)
+  if (site_capacity <= 0 || site_capacity > ((int64_t)1 << 31) - 64 || max_lattices <= 0 || max_lattices > kMaxBatchLattices)
     throw Error{HB_ERR_ARG, "batch capacity out of range"};
-  inv_scale_ = precision == HB_STORE_FP16 ? 1.0f / 1024.0f : 1.0f;
   cap_sites_ = site_capacity;
   np_ = ((site_capacity + 63) / 64) * 64;
   cap_gen_ = std::max<int64_t>(64, general_capacity);
@@ -129,6 +128,8 @@ Batch::Batch(int64_t site_capacity, int64_t general_capacity, int max_lattices, 
   alloc(iolets_, (size_t)max_lat_ * 32 * sizeof(IoletDev), 0);
   alloc(dens_, (size_t)max_lat_ * 32 * sizeof(double), 0);
   alloc(lat_status_, (size_t)max_lat_ * sizeof(int), 0);
+  alloc(macro_list_, (size_t)max_lat_ * sizeof(int), 0);
+  alloc(macro_count_, sizeof(int), 0);
   alloc(rho_, (size_t)np_ * sizeof(double), 0);
   alloc(u_, (size_t)3 * np_ * sizeof(double), 0);
   alloc(wss_, (size_t)np_ * sizeof(double), 0);
@@ -225,7 +226,7 @@ void Batch::clear_member_tables(const BatchMember& m) {
   check(cudaStreamSynchronize(stream_), "clear");
 }
 
-int Batch::add(LatticeTables t, const hb_params& p, int kernel, int wall, uint64_t steps) {
+std::unique_ptr<PreparedLattice> prepare_lattice(LatticeTables t, const hb_params& p, int kernel, int wall, uint64_t steps) {
   if (kernel != kLBGK && kernel != kTRT) throw Error{HB_ERR_UNSUPPORTED, "the batched form runs LBGK or TRT"};
   if (wall != kSBB && wall != kBFL) throw Error{HB_ERR_UNSUPPORTED, "the batched form runs bounce-back or BFL walls"};
   for (int k = 0; k < p.n_inlets + p.n_outlets; k++) {
@@ -235,21 +236,47 @@ int Batch::add(LatticeTables t, const hb_params& p, int kernel, int wall, uint64
   }
   if (!(p.tau > 0.5)) throw Error{HB_ERR_ARG, "tau must exceed 1/2"};
   if (wall == kBFL && t.q.empty()) throw Error{HB_ERR_ARG, "BFL walls need wall distances"};
+  auto prep = std::make_unique<PreparedLattice>();
+  prep->L = build_layout(t, p, wall);
+  prep->t = std::move(t);
+  prep->p = p;
+  prep->kernel = kernel;
+  prep->wall = wall;
+  prep->steps = steps;
+  return prep;
+}
+
+int Batch::add(LatticeTables t, const hb_params& p, int kernel, int wall, uint64_t steps) {
+  auto prep = prepare_lattice(std::move(t), p, kernel, wall, steps);
+  return add(*prep);
+}
+
+int Batch::add(PreparedLattice& prep) {
+  if (prep.taken) throw Error{HB_ERR_ARG, "the prepared lattice was already admitted"};
   if (free_slots_.empty()) throw Error{HB_ERR_OOM, "no free lattice slot in the batch"};
-  auto m = std::make_unique<BatchMember>();
-  m->L = build_layout(t, p, wall);
-  m->site_len = ((m->L.n + 63) / 64) * 64;
-  m->site_base = sites_.take(m->site_len);
-  m->run_base = m->site_base < 0 ? -1 : runs_.take(m->L.runs);
-  m->gen_base = m->run_base < 0 ? -1 : gens_.take(std::max(1, m->L.G));
-  if (m->site_base < 0 || m->run_base < 0 || m->gen_base < 0) {
-    if (m->site_base >= 0) sites_.give(m->site_base, m->site_len);
-    if (m->run_base >= 0) runs_.give(m->run_base, m->L.runs);
+  const int n = prep.L.n;
+  const int64_t site_len = ((n + 63) / 64) * 64;
+  const int64_t site_base = sites_.take(site_len);
+  const int64_t run_base = site_base < 0 ? -1 : runs_.take(prep.L.runs);
+  const int64_t gen_base = run_base < 0 ? -1 : gens_.take(std::max(1, prep.L.G));
+  if (site_base < 0 || run_base < 0 || gen_base < 0) {
+    if (site_base >= 0) sites_.give(site_base, site_len);
+    if (run_base >= 0) runs_.give(run_base, prep.L.runs);
     throw Error{HB_ERR_OOM, "the lattice does not fit in the batch's free capacity"};
   }
+  auto m = std::make_unique<BatchMember>();
+  m->L = std::move(prep.L);
+  prep.taken = true;
+  m->site_len = site_len;
+  m->site_base = site_base;
+  m->run_base = run_base;
+  m->gen_base = gen_base;
+  const hb_params& p = prep.p;
+  const int kernel = prep.kernel, wall = prep.wall;
+  const uint64_t steps = prep.steps;
   m->slot = free_slots_.back();
   free_slots_.pop_back();
-  m->t = std::move(t);
+  m->t = std::move(prep.t);
   m->p = p;
   m->kernel = kernel;
   m->wall = wall;
@@ -267,6 +294,8 @@ int Batch::add(LatticeTables t, const hb_params& p, int kernel, int wall, uint64
   d.t = m->t_first;
   d.t_first = m->t_first;
   d.t_end = m->t_first + steps;
+  d.site_base = m->site_base;
+  d.n_sites = m->L.n;
   d.kernel = kernel;
   d.wall = wall;
   d.io_base = 32 * m->slot;
@@ -304,13 +333,17 @@ int Batch::add(LatticeTables t, const hb_params& p, int kernel, int wall, uint64
   check(cudaMemcpyAsync(cos_.as<BatchCosDev>() + 32 * m->slot, cs.data(), 32 * sizeof(BatchCosDev), cudaMemcpyHostToDevice, stream_),
         "cosine records");
   check(cudaMemsetAsync(lat_status_.as<int>() + m->slot, 0, sizeof(int), stream_), "status");
-  // Equilibrium initial condition in shifted form, in the buffer the next step reads.
-  float geq[Q];
+  // Equilibrium initial condition in shifted form.  The uniform state at rest is
+  // its own post-collision state, so it is written as the distributions the next
+  // step gathers from, and as the iolet ghosts that step reads.
+  float geq[Q], ghost[18];
   {
     const double rho = p.initial_density;
     for (int i = 0; i < Q; i++) geq[i] = (float)(weight(i) * rho - weight(i));
+    for (int d = 1; d < Q; d++) ghost[d - 1] = geq[inv(d)];
   }
-  launch_fill_shift(f_[cur_].p, np_, m->site_base, m->L.n, geq, precision_, inv_scale_, stream_);
+  launch_fill_shift(f_[cur_].p, np_, m->site_base, m->L.n, geq, precision_, stream_);
+  launch_fill_ghost(ghost_[cur_].as<float>(), cap_gen_, m->gen_base, m->L.G, ghost, stream_);
   check(cudaGetLastError(), "initial fill");
   check(cudaStreamSynchronize(stream_), "admission");
   const int slot = m->slot;
@@ -345,6 +378,7 @@ void Batch::capture(int k) {
   const int gen_tiles = (int)((gens_hw + 127) / 128);
   const int bulk_grid = std::max(1, std::min(bulk_tiles, sm_count_ * std::max(1, bb)));
   const int gen_grid = std::max(1, std::min(gen_tiles, sm_count_ * std::max(1, gb)));
+  const int macro_grid = 2 * sm_count_;
   int n_lat = 0;
   for (auto& kv : members_) n_lat = std::max(n_lat, kv.first + 1);
 
@@ -380,19 +414,21 @@ void Batch::capture(int k) {
     b.fout = f_[1 - par].p;
     b.gin = ghost_[par].as<float>();
     b.gout = ghost_[1 - par].as<float>();
-    b.inv_scale = inv_scale_;
     b.lat = lat_.as<BatchLatDev>();
     b.run_lat = run_lat_.as<int>();
     b.g_lat = g_lat_.as<int>();
     b.dens = dens_.as<double>();
     b.lat_status = lat_status_.as<int>();
+    b.macro_list = macro_list_.as<int>();
+    b.macro_count = macro_count_.as<int>();
     b.n_lat = n_lat;
     b.bulk_tiles = bulk_tiles;
     b.gen_tiles = gen_tiles;
-    launch_batch_begin(lat_.p, cos_.p, dens_.as<double>(), n_lat, stream_);
+    launch_batch_begin(lat_.p, cos_.p, dens_.as<double>(), macro_list_.as<int>(), macro_count_.as<int>(), n_lat, stream_);
     cudaEventRecord(fork_, stream_);
     cudaStreamWaitEvent(side_, fork_, 0);
     launch_batch_step(b, precision_, spt_, bulk_block_, bulk_grid, gen_grid, stream_, side_);
+    launch_batch_macro(b, precision_, macro_grid, side_);
     cudaEventRecord(join_, side_);
     cudaStreamWaitEvent(stream_, join_, 0);
   }

@@ -15,6 +15,9 @@
 
 namespace hb {
 
+// One block of the begin kernel serves every lattice slot.
+constexpr int kMaxBatchLattices = 1024;
+
 // First-fit allocator of index ranges [0, capacity).
 class RangeAlloc {
  public:
@@ -30,6 +33,19 @@ class RangeAlloc {
   std::map<int64_t, int64_t> free_;  // start -> length
   std::map<int64_t, int64_t> used_;
 };
+
+// A lattice checked and laid out on the host, ready for upload.
+struct PreparedLattice {
+  LatticeTables t;
+  hb_params p;
+  int kernel = 0, wall = 0;
+  uint64_t steps = 0;
+  Layout L;
+  bool taken = false;
+};
+
+// Host-only: validate the physics the batched form supports and build the layout.
+std::unique_ptr<PreparedLattice> prepare_lattice(LatticeTables t, const hb_params& p, int kernel, int wall, uint64_t steps);
 
 struct BatchMember {
   int slot = -1;
@@ -51,6 +67,8 @@ class Batch {
 
   // Admit a lattice; returns its slot.  Throws Error(HB_ERR_OOM) when it does not fit.
   int add(LatticeTables t, const hb_params& p, int kernel, int wall, uint64_t steps);
+  // Admit a prepared lattice; its contents move into the batch only on success.
+  int add(PreparedLattice& prep);
   void remove(int slot);
   // Run `k` steps of every active member (a captured CUDA graph per block
   // length); returns the slots that finished during the block.
@@ -79,7 +97,6 @@ class Batch {
   void* batch_args_blob(int parity);
 
   int device_, precision_;
-  float inv_scale_;
   int64_t cap_sites_, np_, cap_gen_;
   int max_lat_;
   int64_t run_cap_;
@@ -91,7 +108,7 @@ class Batch {
   DeviceBuffer f_[2], ghost_[2];
   DeviceBuffer meta_, run_off_, run_lat_;
   DeviceBuffer g_site_, g_run_, g_wall_, g_iolet_, g_src_, g_q_, g_nrm_, g_io_, g_cpl_, g_xyz_, g_lat_;
-  DeviceBuffer lat_, cos_, iolets_, dens_, lat_status_, rho_, u_, wss_;
+  DeviceBuffer lat_, cos_, iolets_, dens_, lat_status_, macro_list_, macro_count_, rho_, u_, wss_;
   int cur_ = 0;
   int spt_ = 2, bulk_block_ = 256;
   int sm_count_ = 148;

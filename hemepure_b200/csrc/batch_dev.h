@@ -10,13 +10,14 @@ namespace hb {
 struct BatchLatDev {
   double tau, omega, omega_minus;
   uint64_t t;          // 1-based step of the next step
-  uint64_t t_first;    // the first step after admission reads f directly
+  uint64_t t_first;    // time step at admission
   uint64_t t_end;      // the lattice stops once t reaches t_end
+  int64_t site_base;   // the lattice's sites are [site_base, site_base + n_sites)
+  int n_sites;
   int kernel, wall;
   int io_base;         // 32 iolet entries per lattice
   int active;          // this step runs
-  int direct;          // this step reads pre-collision f
-  int macro;           // this step fills the macroscopic outputs (the last step)
+  int macro;           // this step is the last: k_batch_macro runs it and fills the outputs
   int ran_prev;        // the previous step ran (its t is still to be advanced)
   int pad;
 };
@@ -34,12 +35,13 @@ struct BatchArgs {
   void* fout;
   const float* gin;
   float* gout;
-  float inv_scale;
   BatchLatDev* lat;
   const int* run_lat;   // lattice of each run
   const int* g_lat;     // lattice of each general site
   double* dens;         // [L][32] iolet densities of this step
   int* lat_status;      // [L] StatusBits per lattice
+  int* macro_list;      // lattices in their last step this step (written by k_batch_begin)
+  int* macro_count;
   int n_lat;
   int bulk_tiles;       // tiles of bulk_block*spt sites
   int gen_tiles;
@@ -49,11 +51,17 @@ struct Row19f {
   float v[19];
 };
 
-void launch_batch_begin(void* lat, const void* cos_tab, double* dens, int n_lat, void* stream);
+// One block (n_lat <= 1024): advances time, iolet densities, and the list of
+// lattices in their last step.
+void launch_batch_begin(void* lat, const void* cos_tab, double* dens, int* macro_list, int* macro_count, int n_lat,
+                        void* stream);
+// The last step of the listed lattices, with the macroscopic outputs.
+void launch_batch_macro(const BatchArgs& b, int precision, int grid, void* stream);
+// Iolet ghosts of general slots [base, base + n) set to vals[d-1] for link d.
+void launch_fill_ghost(float* ghost, int64_t pitch, int64_t base, int64_t n, const float vals[18], void* stream);
 void launch_batch_step(const BatchArgs& b, int precision, int spt, int bulk_block, int bulk_grid, int gen_grid,
                        void* bulk_stream, void* gen_stream);
 int batch_occupancy(int precision, int spt, int bulk_block, int* bulk_blocks_per_sm, int* gen_blocks_per_sm);
-void launch_fill_shift(void* out, int64_t np, int64_t base, int64_t n, const float vals[19], int precision, float inv_scale,
-                       void* stream);
+void launch_fill_shift(void* out, int64_t np, int64_t base, int64_t n, const float vals[19], int precision, void* stream);
 
 }  // namespace hb

@@ -343,6 +343,41 @@ int hb_batch_add(hb_batch* b, const hb_lattice_desc* lat, const hb_params* param
   });
 }
 
+struct hb_batch_prep {
+  std::unique_ptr<hb::PreparedLattice> prep;
+};
+
+int hb_batch_prepare_xml(const char* xml_path, int kernel, int wall, uint64_t steps, hb_batch_prep** out) {
+  if (!xml_path || !out) return HB_ERR_ARG;
+  *out = nullptr;
+  return guard(nullptr, [&] {
+    hb::CaseConfig c = hb::read_case(xml_path, kernel);
+    auto h = std::make_unique<hb_batch_prep>();
+    h->prep = hb::prepare_lattice(hb::read_gmy(c.gmy_path), c.params, kernel, wall, steps);
+    *out = h.release();
+    return HB_OK;
+  });
+}
+
+int hb_batch_prep_sites(const hb_batch_prep* prep, int64_t* sites) {
+  if (!prep || !sites || !prep->prep) return HB_ERR_ARG;
+  *sites = prep->prep->L.n;
+  return HB_OK;
+}
+
+int hb_batch_add_prepared(hb_batch* b, hb_batch_prep* prep, int* slot) {
+  if (!b || !prep || !slot || !prep->prep) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    *slot = b->batch->add(*prep->prep);
+    return HB_OK;
+  });
+}
+
+int hb_batch_prep_free(hb_batch_prep* prep) {
+  delete prep;
+  return HB_OK;
+}
+
 int hb_batch_remove(hb_batch* b, int slot) {
   if (!b) return HB_ERR_ARG;
   return guard(nullptr, [&] {

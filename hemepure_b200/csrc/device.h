@@ -91,13 +91,12 @@ void launch_wk3_begin(WK3Dev* wk3, int nwk3, const double* cpl_buf, double* dens
 void launch_equilibrium_f64(double* f, int64_t np, int n, const double feq[19], void* stream);
 void launch_equilibrium_aos_f64(double* f, int n, const double feq[19], void* stream);
 // Shifted low-precision storage (kernels_mixed.cu): g = f - w stored as FP32, or
-// as FP16 scaled by 1/inv_scale; ghosts in FP32.
+// as FP16 holding g * kHalfScale; ghosts in FP32.
 void launch_step_mixed(const StepArgs& a, int precision, const void* fin, void* fout, const float* gin, float* gout,
-                       float inv_scale, int kernel, int wall, bool gather, bool macro, int which, void* stream);
-void launch_to_aos_mixed(const StepArgs& a, int precision, const void* fin, const float* gin, float inv_scale, int wall,
-                         bool gather, const int* st2ref, double* aos, void* stream);
-void launch_from_aos_mixed(const double* aos, const int* st2ref, int n, int64_t np, int precision, void* out,
-                           float inv_scale, void* stream);
+                       int kernel, int wall, bool gather, bool macro, int which, void* stream);
+void launch_to_aos_mixed(const StepArgs& a, int precision, const void* fin, const float* gin, int wall, bool gather,
+                         const int* st2ref, double* aos, void* stream);
+void launch_from_aos_mixed(const double* aos, const int* st2ref, int n, int64_t np, int precision, void* out, void* stream);
 // Conserved sums (density, momentum x/y/z) over n sites in FP64, deterministic:
 // one partial per block of kSumSitesPerBlock sites in `scratch` (4 doubles per
 // block), then the partials in block order into `out` (4 doubles, device).

@@ -14,6 +14,9 @@
 namespace hb {
 
 constexpr int Q = 19;
+// FP16 shifted storage holds (f - w) * kHalfScale: non-equilibrium parts of
+// order 1e-4..1e-2 then sit in FP16's normal range.
+constexpr float kHalfScale = 1024.0f;
 
 // D3Q19 velocity set, weights and inverse directions (src/lb/lattices/D3Q19.cc:15-33).
 HB_HD constexpr int cx(int i) {

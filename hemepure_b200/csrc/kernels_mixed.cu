@@ -25,6 +25,21 @@ __global__ void __launch_bounds__(256) k_bulk_m(const StepArgs a, const MixArgs 
   bulk_site_m<S, K, GATHER, MACRO>(a, m, s, r);
 }
 
+// Two plain bulk sites per thread (s and s + 256 of a 512-site tile), both
+// gathered before either collides: a thread keeps twice the loads in flight,
+// which FP16 storage (2 bytes per load) needs to cover HBM latency.
+template <class S, int K, bool MACRO>
+__global__ void __launch_bounds__(256) k_bulk_m2(const StepArgs a, const MixArgs m) {
+  const int s0 = blockIdx.x * 512 + threadIdx.x, s1 = s0 + 256;
+  const int r0 = s0 < a.n ? __ldg(a.meta + s0) : -1;
+  const int r1 = s1 < a.n ? __ldg(a.meta + s1) : -1;
+  float g0[Q], g1[Q];
+  if (r0 >= 0) gather_bulk_m<S>(a, m, s0, r0, g0);
+  if (r1 >= 0) gather_bulk_m<S>(a, m, s1, r1, g1);
+  if (r0 >= 0) bulk_collide_m<S, K, MACRO>(a, m, s0, g0);
+  if (r1 >= 0) bulk_collide_m<S, K, MACRO>(a, m, s1, g1);
+}
+
 template <class S, int K, int WALL, bool GATHER, bool MACRO>
 __global__ void __launch_bounds__(128) k_general_m(const StepArgs a, const MixArgs m) {
   const int gi = blockIdx.x * blockDim.x + threadIdx.x;
@@ -44,16 +59,19 @@ __global__ void __launch_bounds__(256) k_to_aos_m(const StepArgs a, const MixArg
 }
 
 template <class S>
-__global__ void k_from_aos_m(const double* aos, const int* st2ref, int n, int64_t np, void* out, float inv_scale) {
+__global__ void k_from_aos_m(const double* aos, const int* st2ref, int n, int64_t np, void* out) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= (int64_t)n * Q) return;
   const int s = (int)(k / Q), i = (int)(k % Q);
-  Store<S>::store(out, (int64_t)i * np + s, (float)(aos[(int64_t)st2ref[s] * Q + i] - weight(i)), inv_scale);
+  Store<S>::store(out, (int64_t)i * np + s, (float)(aos[(int64_t)st2ref[s] * Q + i] - weight(i)));
 }
 
 template <class S, int K, int WALL, bool GATHER, bool MACRO>
 void launch_m4(const StepArgs& a, const MixArgs& m, int which, cudaStream_t st) {
-  if ((which & 1) && a.n > 0) k_bulk_m<S, K, GATHER, MACRO><<<(a.n + 255) / 256, 256, 0, st>>>(a, m);
+  if ((which & 1) && a.n > 0) {
+    if (GATHER && sizeof(S) == 2) k_bulk_m2<S, K, MACRO><<<(a.n + 511) / 512, 256, 0, st>>>(a, m);
+    else k_bulk_m<S, K, GATHER, MACRO><<<(a.n + 255) / 256, 256, 0, st>>>(a, m);
+  }
   if ((which & 2) && a.gen.G > 0) k_general_m<S, K, WALL, GATHER, MACRO><<<(a.gen.G + 127) / 128, 128, 0, st>>>(a, m);
 }
 
@@ -98,30 +116,29 @@ void launch_to_aos1(const StepArgs& a, const MixArgs& m, int wall, bool gather, 
 }  // namespace
 
 void launch_step_mixed(const StepArgs& a, int precision, const void* fin, void* fout, const float* gin, float* gout,
-                       float inv_scale, int kernel, int wall, bool gather, bool macro, int which, void* stream) {
-  const MixArgs m{fin, fout, gin, gout, inv_scale};
+                       int kernel, int wall, bool gather, bool macro, int which, void* stream) {
+  const MixArgs m{fin, fout, gin, gout};
   cudaStream_t st = (cudaStream_t)stream;
   if (precision == HB_STORE_FP16) launch_m0<__half>(a, m, kernel, wall, gather, macro, which, st);
   else launch_m0<float>(a, m, kernel, wall, gather, macro, which, st);
 }
 
-void launch_to_aos_mixed(const StepArgs& a, int precision, const void* fin, const float* gin, float inv_scale, int wall,
-                         bool gather, const int* st2ref, double* aos, void* stream) {
-  const MixArgs m{fin, nullptr, gin, nullptr, inv_scale};
+void launch_to_aos_mixed(const StepArgs& a, int precision, const void* fin, const float* gin, int wall, bool gather,
+                         const int* st2ref, double* aos, void* stream) {
+  const MixArgs m{fin, nullptr, gin, nullptr};
   if (a.n <= 0) return;
   cudaStream_t st = (cudaStream_t)stream;
   if (precision == HB_STORE_FP16) launch_to_aos1<__half>(a, m, wall, gather, st2ref, aos, st);
   else launch_to_aos1<float>(a, m, wall, gather, st2ref, aos, st);
 }
 
-void launch_from_aos_mixed(const double* aos, const int* st2ref, int n, int64_t np, int precision, void* out, float inv_scale,
-                           void* stream) {
+void launch_from_aos_mixed(const double* aos, const int* st2ref, int n, int64_t np, int precision, void* out, void* stream) {
   const int64_t tot = (int64_t)n * Q;
   if (tot <= 0) return;
   cudaStream_t st = (cudaStream_t)stream;
   const unsigned blocks = (unsigned)((tot + 255) / 256);
-  if (precision == HB_STORE_FP16) k_from_aos_m<__half><<<blocks, 256, 0, st>>>(aos, st2ref, n, np, out, inv_scale);
-  else k_from_aos_m<float><<<blocks, 256, 0, st>>>(aos, st2ref, n, np, out, inv_scale);
+  if (precision == HB_STORE_FP16) k_from_aos_m<__half><<<blocks, 256, 0, st>>>(aos, st2ref, n, np, out);
+  else k_from_aos_m<float><<<blocks, 256, 0, st>>>(aos, st2ref, n, np, out);
 }
 
 }  // namespace hb

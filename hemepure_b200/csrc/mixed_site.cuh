@@ -19,17 +19,18 @@ struct Store;
 
 template <>
 struct Store<float> {
-  static __device__ __forceinline__ float load(const void* p, int64_t k, float) { return __ldg(static_cast<const float*>(p) + k); }
-  static __device__ __forceinline__ void store(void* p, int64_t k, float v, float) { static_cast<float*>(p)[k] = v; }
+  static __device__ __forceinline__ float load(const void* p, int64_t k) { return __ldg(static_cast<const float*>(p) + k); }
+  static __device__ __forceinline__ void store(void* p, int64_t k, float v) { static_cast<float*>(p)[k] = v; }
 };
 
+// FP16 holds g * kHalfScale; the scale is a power of two, so scaling is exact.
 template <>
 struct Store<__half> {
-  static __device__ __forceinline__ float load(const void* p, int64_t k, float inv_scale) {
-    return __half2float(static_cast<const __half*>(p)[k]) * inv_scale;
+  static __device__ __forceinline__ float load(const void* p, int64_t k) {
+    return __half2float(__ldg(static_cast<const __half*>(p) + k)) * (1.0f / kHalfScale);
   }
-  static __device__ __forceinline__ void store(void* p, int64_t k, float v, float inv_scale) {
-    static_cast<__half*>(p)[k] = __float2half_rn(v / inv_scale);
+  static __device__ __forceinline__ void store(void* p, int64_t k, float v) {
+    static_cast<__half*>(p)[k] = __float2half_rn(v * kHalfScale);
   }
 };
 
@@ -150,11 +151,10 @@ struct MixArgs {
   void* fout;
   const float* gin;
   float* gout;
-  float inv_scale;   // stored value * inv_scale = g (FP16); 1 for FP32
 };
 
 template <class S>
-__device__ __forceinline__ float ldg_s(const MixArgs& m, int64_t k) { return Store<S>::load(m.fin, k, m.inv_scale); }
+__device__ __forceinline__ float ldg_s(const MixArgs& m, int64_t k) { return Store<S>::load(m.fin, k); }
 
 template <class S>
 __device__ __forceinline__ void gather_bulk_m(const StepArgs& a, const MixArgs& m, int s, int r, float* g) {
@@ -225,15 +225,9 @@ __device__ __forceinline__ void flag_unstable_m(const StepArgs& a, const float* 
   if (bad) atomicOr(a.status, kStatusUnstable);
 }
 
-// One plain bulk site s of run r (k_bulk_m, and the batched kernel).
-template <class S, int K, bool GATHER, bool MACRO>
-__device__ __forceinline__ void bulk_site_m(const StepArgs& a, const MixArgs& m, int s, int r) {
-  float g[Q];
-  if (GATHER) gather_bulk_m<S>(a, m, s, r, g);
-  else {
-#pragma unroll
-    for (int i = 0; i < Q; i++) g[i] = ldg_s<S>(m, (int64_t)i * a.np + s);
-  }
+// Collision and store of plain bulk site s from its pre-collision g.
+template <class S, int K, bool MACRO>
+__device__ __forceinline__ void bulk_collide_m(const StepArgs& a, const MixArgs& m, int s, const float* g) {
   flag_unstable_m(a, g);
   float drho, mx, my, mz;
   moments_g(g, drho, mx, my, mz);
@@ -247,7 +241,7 @@ __device__ __forceinline__ void bulk_site_m(const StepArgs& a, const MixArgs& m,
     om = -1.0f / tau;
   }
 #pragma unroll
-  for (int i = 0; i < Q; i++) Store<S>::store(m.fout, (int64_t)i * a.np + s, collide_one_f<K>(a, g, fneq, om, i), m.inv_scale);
+  for (int i = 0; i < Q; i++) Store<S>::store(m.fout, (int64_t)i * a.np + s, collide_one_f<K>(a, g, fneq, om, i));
   if (MACRO) {
     const float rho = 1.0f + drho;
     a.rho[s] = (double)rho;
@@ -256,6 +250,18 @@ __device__ __forceinline__ void bulk_site_m(const StepArgs& a, const MixArgs& m,
     a.u[2 * a.np + s] = (double)(mz / rho);
     a.wss[s] = kNoValue;
   }
+}
+
+// One plain bulk site s of run r (k_bulk_m, and the batched kernel).
+template <class S, int K, bool GATHER, bool MACRO>
+__device__ __forceinline__ void bulk_site_m(const StepArgs& a, const MixArgs& m, int s, int r) {
+  float g[Q];
+  if (GATHER) gather_bulk_m<S>(a, m, s, r, g);
+  else {
+#pragma unroll
+    for (int i = 0; i < Q; i++) g[i] = ldg_s<S>(m, (int64_t)i * a.np + s);
+  }
+  bulk_collide_m<S, K, MACRO>(a, m, s, g);
 }
 
 // One general site gi (k_general_m, and the batched kernel).
@@ -379,7 +385,7 @@ __device__ __forceinline__ void general_site_m(const StepArgs& a, const MixArgs&
     }
   }
 #pragma unroll
-  for (int i = 0; i < Q; i++) Store<S>::store(m.fout, (int64_t)i * a.np + s, out[i], m.inv_scale);
+  for (int i = 0; i < Q; i++) Store<S>::store(m.fout, (int64_t)i * a.np + s, out[i]);
   const int cpl = im ? __ldg(G.cpl + gi) : -1;
   if (cpl >= 0) {
     const IoletDev& I = a.iolets[io];

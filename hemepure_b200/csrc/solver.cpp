@@ -70,7 +70,6 @@ Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& 
     : t_(std::move(tables)), p_(params), opt_(opt) {
   if (opt_.kernel < 0 || opt_.kernel > 2 || opt_.wall < 0 || opt_.wall > 2) throw Error{HB_ERR_ARG, "unknown kernel or wall type"};
   if (opt_.precision < HB_STORE_FP64 || opt_.precision > HB_STORE_FP16) throw Error{HB_ERR_ARG, "unknown storage precision"};
-  inv_scale_ = opt_.precision == HB_STORE_FP16 ? 1.0f / 1024.0f : 1.0f;
   if (opt_.kernel == kLES && opt_.wall == kGZS)
     throw Error{HB_ERR_UNSUPPORTED, "GZS walls with the LES kernel: the virtual-node collision has no relaxation time"};
   if (!(p_.tau > 0.5)) throw Error{HB_ERR_ARG, "tau must exceed 1/2"};
@@ -219,7 +218,7 @@ void Solver::upload() {
     DeviceBuffer aos;
     aos.alloc((size_t)n * Q * sizeof(double));
     launch_equilibrium_aos_f64(aos.as<double>(), n, feq, stream_);
-    launch_from_aos_mixed(aos.as<double>(), st2ref_.as<int>(), n, np, opt_.precision, f_[0].p, inv_scale_, stream_);
+    launch_from_aos_mixed(aos.as<double>(), st2ref_.as<int>(), n, np, opt_.precision, f_[0].p, stream_);
     check(cudaStreamSynchronize(stream_), "initialisation");
   }
   check(cudaGetLastError(), "equilibrium fill");
@@ -341,7 +340,7 @@ void Solver::launch(const StepArgs& a, bool macro, int which, cudaStream_t st) {
     launch_step_f64(a, opt_.kernel, opt_.wall, !direct_, macro, which, 256, 128, st);
   } else {
     launch_step_mixed(a, opt_.precision, f_[cur_].p, f_[1 - cur_].p, ghost_[cur_].as<float>(), ghost_[1 - cur_].as<float>(),
-                      inv_scale_, opt_.kernel, opt_.wall, !direct_, macro, which, st);
+                      opt_.kernel, opt_.wall, !direct_, macro, which, st);
   }
 }
 
@@ -351,7 +350,7 @@ void Solver::to_aos(bool use_prev, double* dev_aos) {
   StepArgs a = args();
   const int b = use_prev ? 1 - cur_ : cur_;
   const bool gather = use_prev ? !prev_direct_ : !direct_;
-  launch_to_aos_mixed(a, opt_.precision, f_[b].p, ghost_[b].as<float>(), inv_scale_, opt_.wall, gather, st2ref_.as<int>(),
+  launch_to_aos_mixed(a, opt_.precision, f_[b].p, ghost_[b].as<float>(), opt_.wall, gather, st2ref_.as<int>(),
                       dev_aos, stream_);
   check(cudaGetLastError(), "to_aos launch");
 }
@@ -510,7 +509,7 @@ void Solver::set_fs(const double* f) {
     DeviceBuffer tmp;
     tmp.alloc((size_t)L_.n * Q * sizeof(double));
     check(cudaMemcpyAsync(tmp.p, f, (size_t)L_.n * Q * sizeof(double), cudaMemcpyHostToDevice, stream_), "f upload");
-    launch_from_aos_mixed(tmp.as<double>(), st2ref_.as<int>(), L_.n, L_.np, opt_.precision, f_[cur_].p, inv_scale_, stream_);
+    launch_from_aos_mixed(tmp.as<double>(), st2ref_.as<int>(), L_.n, L_.np, opt_.precision, f_[cur_].p, stream_);
     check(cudaGetLastError(), "from_aos launch");
     direct_ = true;
     prev_valid_ = false;

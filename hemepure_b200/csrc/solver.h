@@ -112,7 +112,6 @@ class Solver {
   int64_t last_launches_ = 0;
   int64_t dev_bytes_ = 0;
   int status_sticky_ = 0;
-  float inv_scale_ = 1.0f;        // FP16 storage holds g / inv_scale
   bool prev_valid_ = false;
   bool prev_direct_ = false;
   double dt_ = 1.0, dx_ = 1.0;

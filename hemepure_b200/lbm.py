@@ -41,6 +41,7 @@ EXPORTS = [
     "hb_set_time_step", "hb_moment_sums", "hb_moment_sums_noalloc",
     "hb_batch_bytes", "hb_batch_create", "hb_batch_destroy", "hb_batch_add_xml", "hb_batch_add", "hb_batch_remove",
     "hb_batch_run", "hb_batch_get_macro", "hb_batch_member_info", "hb_batch_set_tuning", "hb_batch_stats",
+    "hb_batch_prepare_xml", "hb_batch_prep_sites", "hb_batch_add_prepared", "hb_batch_prep_free",
 ]
 
 
@@ -135,6 +136,10 @@ def library() -> C.CDLL:
     L.hb_batch_member_info.argtypes = [P, I, P, P, P]
     L.hb_batch_set_tuning.argtypes = [P, I, I]
     L.hb_batch_stats.argtypes = [P, P, P, P]
+    L.hb_batch_prepare_xml.argtypes = [C.c_char_p, I, I, U64, C.POINTER(P)]
+    L.hb_batch_prep_sites.argtypes = [P, P]
+    L.hb_batch_add_prepared.argtypes = [P, P, P]
+    L.hb_batch_prep_free.argtypes = [P]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name != "hb_default_options":
@@ -385,6 +390,33 @@ class Geometry:
             pass
 
 
+class PreparedLattice:
+    """A case parsed, its geometry read and its storage layout built on the
+    host, ready for Batch.add_prepared.  Preparation needs no device and releases
+    the interpreter lock, so it runs on worker threads while blocks step."""
+
+    def __init__(self, xml_path: str, kernel: str = "LBGK", wall: str = "SBB", steps: int = 1000):
+        self._h = C.c_void_p()
+        rc = library().hb_batch_prepare_xml(os.fspath(xml_path).encode(), KERNELS[kernel], WALLS[wall], int(steps),
+                                            C.byref(self._h))
+        if rc != HB_OK:
+            raise HemeLBError(rc, last_create_error())
+        n = C.c_int64()
+        library().hb_batch_prep_sites(self._h, C.byref(n))
+        self.sites = int(n.value)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            library().hb_batch_prep_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Batch:
     """Many lattices resident on one GPU, stepped together (the batched form)."""
 
@@ -412,6 +444,13 @@ class Batch:
         slot = C.c_int()
         self._check(library().hb_batch_add_xml(self._b, os.fspath(xml_path).encode(), KERNELS[kernel], WALLS[wall],
                                                int(steps), C.byref(slot)))
+        return int(slot.value)
+
+    def add_prepared(self, prep: "PreparedLattice") -> int:
+        """Admit a prepared lattice (uploads only).  Raises HemeLBError with code
+        -5 when it does not fit yet; the prepared lattice then stays usable."""
+        slot = C.c_int()
+        self._check(library().hb_batch_add_prepared(self._b, prep._h, C.byref(slot)))
         return int(slot.value)
 
     def remove(self, slot: int) -> None:

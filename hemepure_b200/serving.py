@@ -16,7 +16,7 @@ import os
 import tempfile
 import time
 from collections import deque
-from concurrent.futures import ProcessPoolExecutor
+from concurrent.futures import Future, ProcessPoolExecutor, ThreadPoolExecutor
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Sequence, Tuple
 
@@ -39,7 +39,8 @@ class Request:
     admitted: Optional[float] = None
     finished: Optional[float] = None
     result: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
-    status: int = 0
+    status: int = 0          # status bits of the run (1 unstable, 2 iolet radius), or a negative error code
+    error: str = ""
 
     @property
     def latency(self) -> Optional[float]:
@@ -59,15 +60,17 @@ def _make_request(args) -> Tuple[int, str, str, str, int, int, str]:
     kernel = "LBGK" if rng.random() < 0.5 else "TRT"
     tau = float(rng.uniform(0.51, 1.0))
     nu = (tau - 0.5) / 3.0
-    # velocity at Re <= re_max, capped for the lattice's Mach limit
-    u = min(re_max * nu / (2.0 * r), 0.05) * float(rng.uniform(0.5, 1.0))
+    sev = float(rng.uniform(0.5, 0.75))              # stenosis area reduction
+    # peak inflow velocity at Re <= re_max (on the inlet diameter), capped so the
+    # fastest section (the stenosis throat) stays below 0.03 lattice units
+    narrowing = (1.0 - sev) if shape == "stenosis" else 1.0
+    u = min(re_max * nu / (2.0 * r), 0.03 * narrowing) * float(rng.uniform(0.5, 1.0))
     steps = int(rng.integers(step_range[0], step_range[1] + 1))
     ri = max(3, int(round(r)))
     li = max(8, int(round(length)))
     if shape == "pipe":
         v = vessels.Pipe(ri, li)
     elif shape == "stenosis":
-        sev = float(rng.uniform(0.5, 0.75))          # area reduction
         rmin = max(2.0, ri * math.sqrt(1.0 - sev))
         v = vessels.Stenosis(ri, li, rmin, max(4.0, 2.0 * ri))
     else:
@@ -136,13 +139,16 @@ class Tuning:
     table: Dict[str, float] = field(default_factory=dict)
 
 
-def autotune(probe: Sequence[Request], tolerance: float = 1e-4, device: int = 0, block_steps: int = 64,
+def autotune(probe: Sequence[Request], tolerance: float = 1e-4, device: int = 0, block_steps: int = 100,
              site_capacity: Optional[int] = None) -> Tuning:
-    """Pick sites per thread, threads per block and storage precision.
+    """Pick sites per thread, threads per block and storage precision, and
+    measure the batch's capacity in MLUPS.
 
     Precision: FP16 storage is only eligible when the tolerance allows its error
-    (about 1e-3 relative in velocity against FP64); otherwise FP32.  The launch
-    shape is timed on a probe batch holding the given requests."""
+    (about 1e-3 relative in velocity against FP64); otherwise FP32.  Each launch
+    shape is timed on a probe batch holding all the given requests at once (the
+    device time of a block of steps after a warm-up block), so the probe should
+    hold enough sites to fill the device, as a loaded server does."""
     precisions = ["fp32"] + (["fp16"] if tolerance >= 5e-3 else [])
     total = sum(r.sites for r in probe)
     cap = site_capacity or int(total * 1.1) + 64 * len(probe) + 1024
@@ -167,15 +173,32 @@ def autotune(probe: Sequence[Request], tolerance: float = 1e-4, device: int = 0,
     return best
 
 
+def capacity_probe(requests: Sequence[Request], min_sites: int = 8_000_000, max_requests: int = 64) -> List[Request]:
+    """The first requests of the stream whose sites add up to min_sites (a
+    loaded server's resident set), for the autotuner's capacity measurement."""
+    out, n = [], 0
+    for r in requests:
+        if n >= min_sites or len(out) >= max_requests:
+            break
+        out.append(r)
+        n += r.sites
+    return out
+
+
 # ---------------------------------------------------------------------------
 # Server
 # ---------------------------------------------------------------------------
 
 class Server:
-    """Continuous batching of solve requests on one GPU under an HBM budget."""
+    """Continuous batching of solve requests on one GPU under an HBM budget.
+
+    Each request is prepared (case parsed, geometry read, storage layout built)
+    on a pool of host threads as soon as it arrives, while the device steps the
+    resident lattices; admission between blocks is then an upload.  Requests are
+    admitted in arrival order as slots and memory free up."""
 
     def __init__(self, budget_bytes: int, device: int = 0, tuning: Optional[Tuning] = None, block_steps: int = 100,
-                 max_lattices: int = 256, general_fraction: float = 0.6):
+                 max_lattices: int = 256, general_fraction: float = 0.6, prep_workers: int = 0):
         precision = tuning.precision if tuning else "fp32"
         # Largest site capacity whose arena fits the budget.
         lo, hi = 1024, 1 << 31
@@ -192,25 +215,43 @@ class Server:
             self.batch.set_tuning(tuning.sites_per_thread, tuning.block)
         self.block_steps = block_steps
         self.queue: deque = deque()
+        self.prepared: Dict[int, Future] = {}
+        self.pool = ThreadPoolExecutor(max_workers=prep_workers or min(8, os.cpu_count() or 1))
         self.running: Dict[int, Request] = {}
         self.completed: List[Request] = []
         self.site_updates = 0
         self.device_ms = 0.0
+        self.blocks = 0
 
     def submit(self, r: Request) -> None:
+        self.prepared[r.rid] = self.pool.submit(lbm.PreparedLattice, r.xml, r.kernel, r.wall, r.steps)
         self.queue.append(r)
 
     def _admit(self, now: float) -> None:
-        while self.queue and self.queue[0].arrival <= now:
+        while self.queue:
             r = self.queue[0]
+            fut = self.prepared[r.rid]
+            if not fut.done() and self.running:
+                return                     # keep stepping; admit it after the next block
             try:
-                slot = self.batch.add_xml(r.xml, r.kernel, r.wall, r.steps)
+                prep = fut.result()
+            except lbm.HemeLBError as e:   # the case itself is invalid: retire it as failed
+                r.status, r.error = e.code, str(e)
+                r.admitted = r.finished = now
+                self.completed.append(r)
+                self.queue.popleft()
+                del self.prepared[r.rid]
+                continue
+            try:
+                slot = self.batch.add_prepared(prep)
             except lbm.HemeLBError as e:
-                if e.code == -5:      # no room yet: wait for a retirement (FIFO)
+                if e.code == -5:           # no room yet: wait for a retirement (FIFO)
                     if not self.running:
                         raise RuntimeError(f"request {r.rid} ({r.sites} sites) exceeds the whole budget") from e
                     return
                 raise
+            prep.close()
+            del self.prepared[r.rid]
             r.admitted = now
             self.running[slot] = r
             self.queue.popleft()
@@ -218,41 +259,49 @@ class Server:
     def run(self, requests: Sequence[Request], keep_results: bool = False, clock=time.perf_counter) -> None:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         t0 = clock()
-        while pending or self.queue or self.running:
-            now = clock() - t0
-            while pending and pending[0].arrival <= now:
-                self.submit(pending.popleft())
-            self._admit(now)
-            if not self.running:
-                if pending:
-                    time.sleep(max(0.0, min(0.05, pending[0].arrival - (clock() - t0))))
-                continue
-            active = self.batch.stats()[1]
-            done = self.batch.run(self.block_steps)
-            ms = self.batch.stats()[0]
-            self.device_ms += ms
-            self.site_updates += active * self.block_steps
-            now = clock() - t0
-            for slot in done:
-                r = self.running.pop(slot)
-                n, t, st = self.batch.info(slot)
-                r.status = st
-                res = self.batch.macro(slot)
-                if keep_results:
-                    r.result = res
-                r.finished = now
-                self.batch.remove(slot)
-                self.completed.append(r)
+        try:
+            while pending or self.queue or self.running:
+                now = clock() - t0
+                while pending and pending[0].arrival <= now:
+                    self.submit(pending.popleft())
+                self._admit(now)
+                if not self.running:
+                    if pending and not self.queue:
+                        time.sleep(max(0.0, min(0.05, pending[0].arrival - (clock() - t0))))
+                    continue
+                active = self.batch.stats()[1]
+                done = self.batch.run(self.block_steps)
+                ms = self.batch.stats()[0]
+                self.device_ms += ms
+                self.blocks += 1
+                self.site_updates += active * self.block_steps
+                now = clock() - t0
+                for slot in done:
+                    r = self.running.pop(slot)
+                    n, t, st = self.batch.info(slot)
+                    r.status = st
+                    res = self.batch.macro(slot)
+                    if keep_results:
+                        r.result = res
+                    r.finished = now
+                    self.batch.remove(slot)
+                    self.completed.append(r)
+        finally:
+            self.pool.shutdown(wait=True)
         self.wall_s = clock() - t0
 
     def report(self) -> Dict[str, float]:
         lat = np.array([r.latency for r in self.completed])
         work = sum(r.sites * r.steps for r in self.completed)
+        failed = [r for r in self.completed if r.status]
         return {"requests": len(self.completed), "p50_latency_s": float(np.percentile(lat, 50)),
                 "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
                 "aggregate_MLUPS": work / self.wall_s / 1e6, "wall_s": self.wall_s,
                 "device_busy_MLUPS": self.site_updates / (self.device_ms * 1e-3) / 1e6 if self.device_ms else 0.0,
-                "site_capacity": self.site_capacity, "failed": int(sum(1 for r in self.completed if r.status))}
+                "device_busy_fraction": self.device_ms * 1e-3 / self.wall_s if self.wall_s else 0.0,
+                "blocks": self.blocks, "site_capacity": self.site_capacity, "failed": len(failed),
+                "failed_requests": [{"rid": r.rid, "status": r.status, "shape": r.shape, "sites": r.sites}
+                                    for r in failed]}
 
 
 def solve_sequential_fp64(requests: Sequence[Request], device: int = 0) -> Dict[str, float]:
@@ -267,3 +316,40 @@ def solve_sequential_fp64(requests: Sequence[Request], device: int = 0) -> Dict[
         work += r.sites * r.steps
     dt = time.perf_counter() - t0
     return {"requests": len(requests), "MLUPS": work / dt / 1e6, "wall_s": dt}
+
+
+def _main(argv=None) -> None:
+    """Resident-batch probe: the first requests of the seeded stream admitted at
+    once and stepped for a few blocks; prints the device time per block.
+
+        python -m hemepure_b200.serving --requests 8 --blocks 3 --block-steps 20
+    """
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--requests", type=int, default=8)
+    ap.add_argument("--blocks", type=int, default=3)
+    ap.add_argument("--block-steps", type=int, default=20)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"])
+    ap.add_argument("--sites-per-thread", type=int, default=2)
+    ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    reqs = generate_requests(a.requests, a.out, seed=a.seed)
+    total = sum(r.sites for r in reqs)
+    b = lbm.Batch(total + 64 * len(reqs) + 1024, total + 1024, max(8, len(reqs)), precision=a.precision)
+    b.set_tuning(a.sites_per_thread, a.block)
+    for r in reqs:
+        b.add_xml(r.xml, r.kernel, r.wall, 10 ** 9)
+    rows = []
+    for _ in range(a.blocks):
+        b.run(a.block_steps)
+        ms, act, _ = b.stats()
+        rows.append({"block_ms": ms, "active_sites": act, "MLUPS": act * a.block_steps / (ms * 1e-3) / 1e6})
+    print(json.dumps({"requests": len(reqs), "sites": total, "blocks": rows}))
+    b.close()
+
+
+if __name__ == "__main__":
+    _main()

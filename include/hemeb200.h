@@ -207,6 +207,18 @@ int hb_batch_add_xml(hb_batch* b, const char* xml_path, int kernel, int wall, ui
 int hb_batch_add(hb_batch* b, const hb_lattice_desc* lat, const hb_params* params, int kernel, int wall, uint64_t steps,
                  int* slot);
 int hb_batch_remove(hb_batch* b, int slot);
+/* The host half of hb_batch_add_xml, for overlapping admission with running
+ * blocks: parse the case, read the geometry, check the physics is supported and
+ * build the storage layout.  Needs no device, touches no batch, and may run on
+ * any number of threads at once.  hb_batch_add_prepared then only uploads; on
+ * HB_OK the batch has taken the prepared lattice's contents, on any error (e.g.
+ * HB_ERR_OOM, no room yet) they stay for a later attempt.  The caller frees the
+ * object with hb_batch_prep_free either way. */
+typedef struct hb_batch_prep hb_batch_prep;
+int hb_batch_prepare_xml(const char* xml_path, int kernel, int wall, uint64_t steps, hb_batch_prep** out);
+int hb_batch_prep_sites(const hb_batch_prep* prep, int64_t* sites);
+int hb_batch_add_prepared(hb_batch* b, hb_batch_prep* prep, int* slot);
+int hb_batch_prep_free(hb_batch_prep* prep);
 /* Run a block of k steps; the slots that reached their step count are written
  * to finished[0 .. *n_finished) (at most max_finished). */
 int hb_batch_run(hb_batch* b, int k, int* finished, int max_finished, int* n_finished);

@@ -101,3 +101,16 @@ def test_malformed_inputs_are_rejected(tmp_path):
     with pytest.raises(lbm.HemeLBError) as e:
         lbm.read_case(str(xml))
     assert e.value.code == -3
+
+
+def test_batch_preparation_is_host_only(case_dir):
+    """hb_batch_prepare_xml parses, reads and lays out a lattice without a device,
+    and refuses physics the batched form does not run."""
+    xml, gmy, info, kernel, wall, steps = make_small_case(case_dir, "pipe_bfl")
+    prep = lbm.PreparedLattice(xml, kernel, wall, 100)
+    assert prep.sites == info.fluid_sites
+    prep.close()
+    xml, gmy, info, kernel, wall, steps = make_small_case(case_dir, "stenosis")
+    with pytest.raises(lbm.HemeLBError) as e:
+        lbm.PreparedLattice(xml, kernel, wall, 100)     # LBGK+LES is not run batched
+    assert e.value.code == -7

@@ -96,3 +96,23 @@ def test_admission_beyond_capacity_is_refused(mix):
     with pytest.raises(lbm.HemeLBError) as e:
         b.add_xml(xml, kernel, wall, steps)
     assert e.value.code == -5
+
+
+def test_prepared_admission_matches_and_survives_refusal(mix):
+    """A lattice prepared on the host gives the same result as add_xml, and a
+    prepared lattice refused for lack of room can be admitted later."""
+    name, xml, kernel, wall, steps = mix[0]
+    ref = run_alone(xml, kernel, wall, steps)
+    prep = lbm.PreparedLattice(xml, kernel, wall, steps)
+    small = lbm.Batch(prep.sites // 2, prep.sites // 2, 2)
+    with pytest.raises(lbm.HemeLBError) as e:
+        small.add_prepared(prep)
+    assert e.value.code == -5
+    b = lbm.Batch(400_000, 200_000, 8)
+    slot = b.add_prepared(prep)
+    prep.close()
+    done = []
+    while not done:
+        done = b.run(64)
+    for a, m in zip(ref, b.macro(slot)):
+        assert np.array_equal(a, m)
