@@ -72,7 +72,7 @@ int64_t Batch::bytes_for(int64_t site_capacity, int64_t general_capacity, int ma
   const int64_t elem = precision == HB_STORE_FP16 ? 2 : 4;
   const int64_t runs = std::max<int64_t>(1024, site_capacity / 4);
   const int64_t g = std::max<int64_t>(64, general_capacity);
-  return 2 * 19 * np * elem + 2 * 18 * g * 4 + np * 4 + runs * 21 * 4 + g * (4 * 8 + 18 * 8 + 3 * 8) +
+  return 2 * 19 * np * elem + 2 * 18 * g * 4 + 5 * g * 4 + np * 4 + runs * 20 * 4 + g * (4 * 8 + 18 * 8 + 3 * 8) +
          np * 5 * 8 + (int64_t)max_lattices * (sizeof(BatchLatDev) + 32 * (sizeof(BatchCosDev) + sizeof(IoletDev) + 8) + 4);
 }
 
@@ -89,14 +89,12 @@ Batch::Batch(int64_t site_capacity, int64_t general_capacity, int max_lattices, 
   run_cap_ = std::max<int64_t>(1024, site_capacity / 4);
   sites_.reset(np_);
   gens_.reset(cap_gen_);
+  iols_.reset(cap_gen_);
   runs_.reset(run_cap_);
   for (int s = max_lat_ - 1; s >= 0; s--) free_slots_.push_back(s);
   check(cudaSetDevice(device_), "cudaSetDevice");
   cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_);
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-  check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
-  check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
-  check(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaEventCreate(&ev0_), "cudaEventCreate");
   check(cudaEventCreate(&ev1_), "cudaEventCreate");
   const size_t elem = precision == HB_STORE_FP16 ? 2 : 4;
@@ -111,7 +109,6 @@ Batch::Batch(int64_t site_capacity, int64_t general_capacity, int max_lattices, 
   }
   alloc(meta_, (size_t)np_ * sizeof(int), 0xFF);
   alloc(run_off_, (size_t)run_cap_ * 20 * sizeof(int), 0);
-  alloc(run_lat_, (size_t)run_cap_ * sizeof(int), 0xFF);
   alloc(g_site_, (size_t)cap_gen_ * sizeof(int), 0);
   alloc(g_run_, (size_t)cap_gen_ * sizeof(int), 0xFF);
   alloc(g_wall_, (size_t)cap_gen_ * sizeof(uint32_t), 0);
@@ -130,6 +127,8 @@ Batch::Batch(int64_t site_capacity, int64_t general_capacity, int max_lattices, 
   alloc(lat_status_, (size_t)max_lat_ * sizeof(int), 0);
   alloc(macro_list_, (size_t)max_lat_ * sizeof(int), 0);
   alloc(macro_count_, sizeof(int), 0);
+  alloc(io_moments_, (size_t)4 * cap_gen_ * sizeof(float), 0);
+  alloc(iol_list_, (size_t)cap_gen_ * sizeof(int), 0xFF);
   alloc(rho_, (size_t)np_ * sizeof(double), 0);
   alloc(u_, (size_t)3 * np_ * sizeof(double), 0);
   alloc(wss_, (size_t)np_ * sizeof(double), 0);
@@ -138,11 +137,9 @@ Batch::Batch(int64_t site_capacity, int64_t general_capacity, int max_lattices, 
 
 Batch::~Batch() {
   if (stream_) cudaStreamSynchronize(stream_);
-  if (side_) cudaStreamSynchronize(side_);
   if (graph_) cudaGraphExecDestroy(graph_);
-  for (cudaEvent_t e : {fork_, join_, ev0_, ev1_})
+  for (cudaEvent_t e : {ev0_, ev1_})
     if (e) cudaEventDestroy(e);
-  if (side_) cudaStreamDestroy(side_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -193,9 +190,10 @@ void Batch::write_member_tables(const BatchMember& m) {
   std::vector<int> meta(m.site_len, -1);
   for (int s = 0; s < n; s++) meta[s] = L.meta[s] >= 0 ? L.meta[s] + (int)m.run_base : L.meta[s] - (int)m.gen_base;
   put(meta_, m.site_base, meta.data(), (int64_t)meta.size(), stream_);
-  put(run_off_, m.run_base * 20, L.run_off.data(), (int64_t)L.run_off.size(), stream_);
-  std::vector<int> rl(L.runs, m.slot);
-  put(run_lat_, m.run_base, rl.data(), (int64_t)rl.size(), stream_);
+  // Run rows: the offsets of the layout, and the member's slot in the spare last entry.
+  std::vector<int> rows(L.run_off);
+  for (int r = 0; r < L.runs; r++) rows[(size_t)r * 20 + 19] = m.slot;
+  put(run_off_, m.run_base * 20, rows.data(), (int64_t)rows.size(), stream_);
   if (G > 0) {
     std::vector<int> site(G), run(G), src((size_t)18 * G), lat(G, m.slot), cpl(G, -1);
     for (int g = 0; g < G; g++) {
@@ -214,12 +212,18 @@ void Batch::write_member_tables(const BatchMember& m) {
     put_rows(g_q_, cap_gen_, m.gen_base, L.g_q.data(), G, 18, stream_);
     put_rows(g_nrm_, cap_gen_, m.gen_base, L.g_nrm.data(), G, 3, stream_);
     put_rows(g_xyz_, cap_gen_, m.gen_base, L.g_xyz.data(), G, 3, stream_);
+    std::vector<int> iol;
+    for (int g = 0; g < G; g++)
+      if (L.g_iolet[g]) iol.push_back(g + (int)m.gen_base);
+    put(iol_list_, m.iol_base, iol.data(), (int64_t)iol.size(), stream_);
   }
 }
 
 void Batch::clear_member_tables(const BatchMember& m) {
   check(cudaMemsetAsync(meta_.as<int>() + m.site_base, 0xFF, (size_t)m.site_len * sizeof(int), stream_), "clear");
   check(cudaMemsetAsync(g_lat_.as<int>() + m.gen_base, 0xFF, (size_t)std::max(1, m.L.G) * sizeof(int), stream_), "clear");
+  check(cudaMemsetAsync(iol_list_.as<int>() + m.iol_base, 0xFF, (size_t)std::max<int64_t>(1, m.iol_len) * sizeof(int), stream_),
+        "clear");
   BatchLatDev z;
   std::memset(&z, 0, sizeof(z));
   check(cudaMemcpyAsync(lat_.as<BatchLatDev>() + m.slot, &z, sizeof(z), cudaMemcpyHostToDevice, stream_), "clear");
@@ -259,9 +263,13 @@ int Batch::add(PreparedLattice& prep) {
   const int64_t site_base = sites_.take(site_len);
   const int64_t run_base = site_base < 0 ? -1 : runs_.take(prep.L.runs);
   const int64_t gen_base = run_base < 0 ? -1 : gens_.take(std::max(1, prep.L.G));
-  if (site_base < 0 || run_base < 0 || gen_base < 0) {
+  int64_t iol_len = 0;
+  for (int g = 0; g < prep.L.G; g++) iol_len += prep.L.g_iolet[g] ? 1 : 0;
+  const int64_t iol_base = gen_base < 0 ? -1 : iols_.take(std::max<int64_t>(1, iol_len));
+  if (site_base < 0 || run_base < 0 || gen_base < 0 || iol_base < 0) {
     if (site_base >= 0) sites_.give(site_base, site_len);
     if (run_base >= 0) runs_.give(run_base, prep.L.runs);
+    if (gen_base >= 0) gens_.give(gen_base, std::max(1, prep.L.G));
     throw Error{HB_ERR_OOM, "the lattice does not fit in the batch's free capacity"};
   }
   auto m = std::make_unique<BatchMember>();
@@ -271,6 +279,8 @@ int Batch::add(PreparedLattice& prep) {
   m->site_base = site_base;
   m->run_base = run_base;
   m->gen_base = gen_base;
+  m->iol_base = iol_base;
+  m->iol_len = iol_len;
   const hb_params& p = prep.p;
   const int kernel = prep.kernel, wall = prep.wall;
   const uint64_t steps = prep.steps;
@@ -360,6 +370,7 @@ void Batch::remove(int slot) {
   sites_.give(m.site_base, m.site_len);
   runs_.give(m.run_base, m.L.runs);
   gens_.give(m.gen_base, std::max(1, m.L.G));
+  iols_.give(m.iol_base, std::max<int64_t>(1, m.iol_len));
   free_slots_.push_back(slot);
   members_.erase(it);
   dirty_ = true;
@@ -370,15 +381,16 @@ void Batch::capture(int k) {
     cudaGraphExecDestroy(graph_);
     graph_ = nullptr;
   }
-  int bb = 0, gb = 0;
-  if (batch_occupancy(precision_, spt_, bulk_block_, &bb, &gb) != 0) throw Error{HB_ERR_CUDA, "occupancy query failed"};
+  int per_sm = 0;
+  if (batch_occupancy(precision_, spt_, bulk_block_, &per_sm) != 0) throw Error{HB_ERR_CUDA, "occupancy query failed"};
   const int64_t sites_hw = sites_.high_water(), gens_hw = gens_.high_water();
   const int span = bulk_block_ * spt_;
   const int bulk_tiles = (int)((sites_hw + span - 1) / span);
-  const int gen_tiles = (int)((gens_hw + 127) / 128);
-  const int bulk_grid = std::max(1, std::min(bulk_tiles, sm_count_ * std::max(1, bb)));
-  const int gen_grid = std::max(1, std::min(gen_tiles, sm_count_ * std::max(1, gb)));
+  const int gen_tiles = (int)((gens_hw + bulk_block_ - 1) / bulk_block_);
+  const int grid = std::max(1, std::min(bulk_tiles + gen_tiles, sm_count_ * std::max(1, per_sm)));
   const int macro_grid = 2 * sm_count_;
+  const int64_t iols_hw = iols_.high_water();
+  const int ghost_grid = std::max(1, std::min((int)((iols_hw + 127) / 128), 4 * sm_count_));
   int n_lat = 0;
   for (auto& kv : members_) n_lat = std::max(n_lat, kv.first + 1);
 
@@ -415,22 +427,21 @@ void Batch::capture(int k) {
     b.gin = ghost_[par].as<float>();
     b.gout = ghost_[1 - par].as<float>();
     b.lat = lat_.as<BatchLatDev>();
-    b.run_lat = run_lat_.as<int>();
     b.g_lat = g_lat_.as<int>();
     b.dens = dens_.as<double>();
     b.lat_status = lat_status_.as<int>();
     b.macro_list = macro_list_.as<int>();
     b.macro_count = macro_count_.as<int>();
+    b.io_moments = io_moments_.as<float>();
+    b.iol_list = iol_list_.as<int>();
+    b.iol_count = (int)iols_hw;
     b.n_lat = n_lat;
     b.bulk_tiles = bulk_tiles;
     b.gen_tiles = gen_tiles;
     launch_batch_begin(lat_.p, cos_.p, dens_.as<double>(), macro_list_.as<int>(), macro_count_.as<int>(), n_lat, stream_);
-    cudaEventRecord(fork_, stream_);
-    cudaStreamWaitEvent(side_, fork_, 0);
-    launch_batch_step(b, precision_, spt_, bulk_block_, bulk_grid, gen_grid, stream_, side_);
-    launch_batch_macro(b, precision_, macro_grid, side_);
-    cudaEventRecord(join_, side_);
-    cudaStreamWaitEvent(stream_, join_, 0);
+    launch_batch_step(b, precision_, spt_, bulk_block_, grid, stream_);
+    launch_batch_ghosts(b, precision_, ghost_grid, stream_);
+    launch_batch_macro(b, precision_, macro_grid, stream_);
   }
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(stream_, &g);

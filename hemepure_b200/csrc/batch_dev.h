@@ -36,15 +36,17 @@ struct BatchArgs {
   const float* gin;
   float* gout;
   BatchLatDev* lat;
-  const int* run_lat;   // lattice of each run
   const int* g_lat;     // lattice of each general site
   double* dens;         // [L][32] iolet densities of this step
   int* lat_status;      // [L] StatusBits per lattice
   int* macro_list;      // lattices in their last step this step (written by k_batch_begin)
   int* macro_count;
+  float* io_moments;    // [4][G] pre-collision density and velocity of records with iolet links
   int n_lat;
-  int bulk_tiles;       // tiles of bulk_block*spt sites
-  int gen_tiles;
+  int bulk_tiles;       // tiles of block*spt sites
+  int gen_tiles;        // tiles of block boundary records
+  const int* iol_list;  // boundary records with iolet links (-1: free entry)
+  int iol_count;        // entries of iol_list in use (high-water mark)
 };
 
 struct Row19f {
@@ -55,13 +57,15 @@ struct Row19f {
 // lattices in their last step.
 void launch_batch_begin(void* lat, const void* cos_tab, double* dens, int* macro_list, int* macro_count, int n_lat,
                         void* stream);
+// Iolet ghosts of the records the step kernel relaxed (after it, same stream).
+void launch_batch_ghosts(const BatchArgs& b, int precision, int grid, void* stream);
 // The last step of the listed lattices, with the macroscopic outputs.
 void launch_batch_macro(const BatchArgs& b, int precision, int grid, void* stream);
 // Iolet ghosts of general slots [base, base + n) set to vals[d-1] for link d.
 void launch_fill_ghost(float* ghost, int64_t pitch, int64_t base, int64_t n, const float vals[18], void* stream);
-void launch_batch_step(const BatchArgs& b, int precision, int spt, int bulk_block, int bulk_grid, int gen_grid,
-                       void* bulk_stream, void* gen_stream);
-int batch_occupancy(int precision, int spt, int bulk_block, int* bulk_blocks_per_sm, int* gen_blocks_per_sm);
+// One step of all running lattices not in their last step (persistent kernel).
+void launch_batch_step(const BatchArgs& b, int precision, int spt, int block, int grid, void* stream);
+int batch_occupancy(int precision, int spt, int block, int* blocks_per_sm);
 void launch_fill_shift(void* out, int64_t np, int64_t base, int64_t n, const float vals[19], int precision, void* stream);
 
 }  // namespace hb

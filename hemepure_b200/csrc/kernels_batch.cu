@@ -5,10 +5,10 @@
 // so the single-lattice gather rules apply unchanged.  Per-lattice parameters
 // (relaxation times, time step, iolets, flags) live in device memory and are
 // advanced by k_batch_begin, so a captured CUDA graph of a block of steps can be
-// replayed without host involvement.  The step is two persistent kernels over
-// the whole arena, one for plain bulk sites (bandwidth-bound) and one for
-// boundary sites (latency-bound), launched side by side; each loops over tiles
-// of the arena with a grid sized to the SM count.  A lattice's last step, which
+// replayed without host involvement.  The step is one persistent kernel over the
+// whole arena whose blocks interleave tiles of plain bulk sites (bandwidth-bound)
+// with tiles of boundary records (latency-bound), so both kinds of work share
+// every SM.  A lattice's last step, which
 // also fills its macroscopic outputs, is run instead by k_batch_macro over the
 // short list k_batch_begin builds, so the step kernels carry no output path.
 // A newly admitted lattice starts from equilibrium in both its distributions and
@@ -33,56 +33,222 @@ __device__ __forceinline__ void patch(StepArgs& a, const BatchLatDev& d, int l, 
   a.status = b.lat_status + l;
 }
 
-template <class S, int SPT>
-__global__ void __launch_bounds__(256) k_batch_bulk(const BatchArgs b) {
-  const MixArgs m{b.fin, b.fout, b.gin, b.gout};
-  const int span = blockDim.x * SPT;
-  for (int tile = blockIdx.x; tile < b.bulk_tiles; tile += gridDim.x) {
-    // All SPT sites are gathered before any collides, so their loads overlap.
-    int s[SPT], l[SPT];
-    float g[SPT][Q];
+// Relax the gathered shifted distributions g in place (LBGK, or TRT by pairs of
+// opposite directions, in the arithmetic of collide_one_f), flagging instability
+// in the lattice's status word.  Returns the pre-collision moments.
+__device__ __forceinline__ void relax_inplace(float* g, int* status, bool trt, float om, float omm, float& drho,
+                                              float& mx, float& my, float& mz) {
+  flag_unstable_status(g, status);
+  moments_g(g, drho, mx, my, mz);
+  const GeqF geq(drho, mx, my, mz);
+  if (trt) {
+    g[0] = g[0] + om * (g[0] - geq(0));
 #pragma unroll
-    for (int k = 0; k < SPT; k++) {
-      s[k] = tile * span + k * blockDim.x + threadIdx.x;
-      l[k] = -1;
-      if (s[k] >= b.base.n) continue;
-      const int r = __ldg(b.base.meta + s[k]);
-      if (r < 0) continue;
-      const int lk = __ldg(b.run_lat + r);
-      if (!b.lat[lk].active || b.lat[lk].macro) continue;
-      l[k] = lk;
-      gather_bulk_m<S>(b.base, m, s[k], r, g[k]);
+    for (int i = 1; i < Q; i += 2) {
+      const int j = i + 1;  // inv(i) for odd i
+      const float fi = g[i] - geq(i), fj = g[j] - geq(j);
+      const float gi = g[i] + 0.5f * om * (fi + fj) + 0.5f * omm * (fi - fj);
+      const float gj = g[j] + 0.5f * om * (fj + fi) + 0.5f * omm * (fj - fi);
+      g[i] = gi;
+      g[j] = gj;
     }
+  } else {
 #pragma unroll
-    for (int k = 0; k < SPT; k++) {
-      if (l[k] < 0) continue;
-      const BatchLatDev d = b.lat[l[k]];
-      StepArgs a = b.base;
-      patch(a, d, l[k], b);
-      if (d.kernel == kTRT) bulk_collide_m<S, kTRT, false>(a, m, s[k], g[k]);
-      else bulk_collide_m<S, kLBGK, false>(a, m, s[k], g[k]);
+    for (int i = 0; i < Q; i++) g[i] = g[i] + (g[i] - geq(i)) * om;
+  }
+}
+
+// Gather of a boundary record with the wall rule chosen at run time (SBB or
+// BFL); the rules are those of gather_general_m.  Every load depends only on
+// the record's metadata and run offsets, so all are in flight together: on a
+// BFL link the value at the site is read whether or not the cut distance
+// selects it.
+template <class S>
+__device__ __forceinline__ void gather_general_rt(const StepArgs& a, const MixArgs& m, int gi, int s, uint32_t wm,
+                                                  uint32_t im, int run, const int* off, bool bfl, float* g) {
+  const GeneralDev& G = a.gen;
+  g[0] = ldg_s<S>(m, s);
+#pragma unroll
+  for (int i = 1; i < Q; i++) {
+    const int d = inv(i);
+    const bool bw = (wm >> (d - 1)) & 1u, bi = (im >> (d - 1)) & 1u;
+    if (bi) {
+      g[i] = __ldg(m.gin + (int64_t)(d - 1) * G.G + gi);
+    } else if (bw) {
+      const float fd = ldg_s<S>(m, (int64_t)d * a.np + s);
+      const bool wi = (wm >> (i - 1)) & 1u;
+      if (bfl && !wi) {
+        const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
+        const float fi = ldg_s<S>(m, (int64_t)i * a.np + s);
+        if (q < 0.5f) g[i] = fd;
+        else g[i] = (fd + (2.0f * q - 1.0f) * fi) / (2.0f * q);
+      } else {
+        g[i] = fd;
+      }
+    } else {
+      const int src = run >= 0 ? s + off[i] : __ldg(G.src + (int64_t)(i - 1) * G.G + gi);
+      g[i] = ldg_s<S>(m, (int64_t)i * a.np + src);
+    }
+  }
+  if (bfl && wm) {
+#pragma unroll
+    for (int d = 1; d < Q; d++) {
+      const int i = inv(d);
+      if (((wm >> (d - 1)) & 1u) && !((wm >> (i - 1)) & 1u)) {
+        const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
+        if (q < 0.5f) g[i] = 2.0f * q * g[i] + (1.0f - 2.0f * q) * g[d];
+      }
     }
   }
 }
 
+__device__ __forceinline__ bool lattice_steps(const BatchArgs& b, int l) {
+  return b.lat[l].active && !b.lat[l].macro;
+}
+
+// A tile of boundary records, one per thread (walls SBB/BFL, LBGK/TRT).  A
+// record with iolet links also leaves its pre-collision density and velocity
+// for k_batch_ghosts, which produces its iolet ghosts after the step: kept out
+// of the step kernel, that rarely taken path does not set its register budget.
 template <class S>
-__global__ void __launch_bounds__(128) k_batch_general(const BatchArgs b) {
+__device__ __forceinline__ void batch_general_tile(const BatchArgs& b, const MixArgs& m, int tile) {
+  const int gi = tile * blockDim.x + threadIdx.x;
+  if (gi >= b.base.gen.G) return;
+  const GeneralDev& G = b.base.gen;
+  const int l = __ldg(b.g_lat + gi);
+  if (l < 0) return;  // a free boundary slot
+  const int s = __ldg(G.site + gi);
+  const uint32_t wm = __ldg(G.wall + gi), im = __ldg(G.iolet + gi);
+  const int run = __ldg(G.run + gi);
+  int off[20];
+  if (run >= 0) run_offsets(b.base, run, off);
+  if (!lattice_steps(b, l)) return;
+  const BatchLatDev& d = b.lat[l];
+  float g[Q];
+  gather_general_rt<S>(b.base, m, gi, s, wm, im, run, off, d.wall == kBFL, g);
+  float drho, mx, my, mz;
+  relax_inplace(g, b.lat_status + l, d.kernel == kTRT, (float)d.omega, (float)d.omega_minus, drho, mx, my, mz);
+#pragma unroll
+  for (int i = 0; i < Q; i++) Store<S>::store(m.fout, (int64_t)i * b.base.np + s, g[i]);
+  if (im) {
+    const float rho = 1.0f + drho;
+    b.io_moments[gi] = rho;
+    b.io_moments[G.G + gi] = mx / rho;
+    b.io_moments[2 * (int64_t)G.G + gi] = my / rho;
+    b.io_moments[3 * (int64_t)G.G + gi] = mz / rho;
+  }
+}
+
+// A tile of SPT * blockDim sites, plain bulk ones taken.  The run row carries
+// the lattice slot in its spare last entry, so the site's run offsets and its
+// lattice come in one load; all SPT sites of a thread are gathered before any
+// relaxes, so their loads are in flight together.
+template <class S, int SPT>
+__device__ __forceinline__ void batch_bulk_tile(const BatchArgs& b, const MixArgs& m, int tile) {
+  int s[SPT], l[SPT];
+  float g[SPT][Q];
+#pragma unroll
+  for (int k = 0; k < SPT; k++) {
+    s[k] = (tile * SPT + k) * blockDim.x + threadIdx.x;
+    l[k] = -1;
+    if (s[k] >= b.base.n) continue;
+    const int r = __ldg(b.base.meta + s[k]);
+    if (r < 0) continue;
+    int off[20];
+    run_offsets(b.base, r, off);
+    if (!lattice_steps(b, off[19])) continue;
+    l[k] = off[19];
+    g[k][0] = ldg_s<S>(m, s[k]);
+#pragma unroll
+    for (int i = 1; i < Q; i++) g[k][i] = ldg_s<S>(m, (int64_t)i * b.base.np + (s[k] + off[i]));
+  }
+#pragma unroll
+  for (int k = 0; k < SPT; k++) {
+    if (l[k] < 0) continue;
+    const BatchLatDev& d = b.lat[l[k]];
+    float drho, mx, my, mz;
+    relax_inplace(g[k], b.lat_status + l[k], d.kernel == kTRT, (float)d.omega, (float)d.omega_minus, drho, mx, my, mz);
+#pragma unroll
+    for (int i = 0; i < Q; i++) Store<S>::store(m.fout, (int64_t)i * b.base.np + s[k], g[k][i]);
+  }
+}
+
+// One time step of every running lattice except those in their last step: a
+// persistent kernel.  Block j takes boundary tiles j, j + grid, ... and bulk
+// tiles j, j + grid, ..., interleaving the two in proportion, so at any moment
+// the SMs mix latency-bound boundary work with bandwidth-bound bulk work (the
+// assignment is static: no counter, no block-wide barrier).  The kernel is
+// latency-bound, so warps per SM set its speed: with one site per thread it is
+// held to 64 registers (four 256-thread blocks per SM; the boundary path spills
+// ~100 bytes to L1, measured 6-11% faster than 80 registers and three blocks),
+// with two sites per thread to 80 registers (tighter bounds spill the second
+// site's values).
+template <class S, int SPT>
+__global__ void __launch_bounds__(256, SPT == 1 ? 4 : 3) k_batch_step(const BatchArgs b) {
   const MixArgs m{b.fin, b.fout, b.gin, b.gout};
-  for (int tile = blockIdx.x; tile < b.gen_tiles; tile += gridDim.x) {
-    const int gi = tile * blockDim.x + threadIdx.x;
-    if (gi >= b.base.gen.G) continue;
-    const int l = __ldg(b.g_lat + gi);
-    if (l < 0) continue;  // a free general slot
-    const BatchLatDev d = b.lat[l];
-    if (!d.active || d.macro) continue;
-    StepArgs a = b.base;
-    patch(a, d, l, b);
-    if (d.kernel == kTRT) {
-      if (d.wall == kBFL) general_site_m<S, kTRT, kBFL, true, false>(a, m, gi);
-      else general_site_m<S, kTRT, kSBB, true, false>(a, m, gi);
+  const int j = blockIdx.x, grid = gridDim.x;
+  const int n_gen = j < b.gen_tiles ? (b.gen_tiles - j + grid - 1) / grid : 0;
+  const int n_bulk = j < b.bulk_tiles ? (b.bulk_tiles - j + grid - 1) / grid : 0;
+  int done_gen = 0, done_bulk = 0;
+  while (done_gen < n_gen || done_bulk < n_bulk) {
+    // the boundary share so far stays at or below its proportion
+    const bool gen_next =
+        done_gen < n_gen && (done_bulk >= n_bulk || (int64_t)done_gen * n_bulk <= (int64_t)done_bulk * n_gen);
+    if (gen_next) {
+      batch_general_tile<S>(b, m, j + done_gen * grid);
+      done_gen++;
     } else {
-      if (d.wall == kBFL) general_site_m<S, kLBGK, kBFL, true, false>(a, m, gi);
-      else general_site_m<S, kLBGK, kSBB, true, false>(a, m, gi);
+      batch_bulk_tile<S, SPT>(b, m, j + done_bulk * grid);
+      done_bulk++;
+    }
+  }
+}
+
+// Iolet ghosts of the boundary records stepped by k_batch_step: the Nash
+// zeroth-order pressure and Ladd velocity rules of general_site_m, from the
+// record's post-collision values (in fout) and its pre-collision density and
+// velocity (io_moments).
+template <class S>
+__global__ void __launch_bounds__(128) k_batch_ghosts(const BatchArgs b) {
+  const GeneralDev& G = b.base.gen;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < b.iol_count; k += gridDim.x * blockDim.x) {
+    const int gi = __ldg(b.iol_list + k);
+    if (gi < 0) continue;
+    const uint32_t im = __ldg(G.iolet + gi);
+    const int l = __ldg(b.g_lat + gi);
+    if (l < 0) continue;
+    const BatchLatDev& d = b.lat[l];
+    if (!d.active || d.macro) continue;
+    const int s = __ldg(G.site + gi);
+    const float rho = b.io_moments[gi], ux = b.io_moments[G.G + gi], uy = b.io_moments[2 * (int64_t)G.G + gi],
+                uz = b.io_moments[3 * (int64_t)G.G + gi];
+    const int io = __ldg(G.io + gi);
+    const IoletDev& I = b.base.iolets[32 * (int64_t)l + io];
+    const double pos[3] = {(double)__ldg(G.xyz + gi), (double)__ldg(G.xyz + G.G + gi), (double)__ldg(G.xyz + 2 * G.G + gi)};
+    const uint64_t t = (uint64_t)(unsigned int)d.t;
+#pragma unroll
+    for (int k = 1; k < Q; k++) {
+      if (!((im >> (k - 1)) & 1u)) continue;
+      float v;
+      if (I.kind == kParabolic) {
+        const double hw[3] = {pos[0] + 0.5 * cx(k), pos[1] + 0.5 * cy(k), pos[2] + 0.5 * cz(k)};
+        float w[3];
+        if (!parabolic_f(I, hw, t, w)) {
+          atomicOr(b.lat_status + l, kStatusIoletRadius);
+          w[0] = w[1] = w[2] = 0.0f;
+        }
+        const float corr = 2.0f * wf(k) * rho * (w[0] * cx(k) + w[1] * cy(k) + w[2] * cz(k)) * 3.0f;
+        v = Store<S>::load(b.fout, (int64_t)k * b.base.np + s) - corr;
+      } else {
+        const double rb = b.dens[32 * (int64_t)l + io];
+        const float drb = (float)(rb - 1.0);
+        const float rbf = (float)rb;
+        const float nx = (float)I.nrm_f[0], ny = (float)I.nrm_f[1], nz = (float)I.nrm_f[2];
+        const float comp = ux * nx + uy * ny + uz * nz;
+        const GeqF gq(drb, nx * comp * rbf, ny * comp * rbf, nz * comp * rbf);
+        v = gq(inv(k));
+      }
+      b.gout[(int64_t)(k - 1) * G.G + gi] = v;
     }
   }
 }
@@ -117,41 +283,46 @@ __global__ void __launch_bounds__(128) k_batch_macro(const BatchArgs b) {
   }
 }
 
-// One block, one thread per lattice: advance the time of lattices that ran,
-// decide which run this step, compute their cosine iolet densities for this step
-// (InOutLetCosine::GetDensity at the 0-indexed step, BoundaryValues.cc:211-214),
-// and list the lattices whose last step this is.
+// One block, one warp per lattice: advance the time of lattices that ran,
+// decide which run this step, list the lattices whose last step this is, and
+// compute their cosine iolet densities for this step, one lane per iolet entry
+// (InOutLetCosine::GetDensity at the 0-indexed step, BoundaryValues.cc:211-214).
 __global__ void __launch_bounds__(1024) k_batch_begin(BatchLatDev* lat, const BatchCosDev* cos_tab, double* dens,
                                                       int* macro_list, int* macro_count, int n_lat) {
   __shared__ int listed;
   if (threadIdx.x == 0) listed = 0;
   __syncthreads();
-  const int l = threadIdx.x;
-  if (l < n_lat) {
-    BatchLatDev d = lat[l];
-    if (d.ran_prev) d.t++;
-    d.active = d.t < d.t_end;
-    d.macro = d.active && (d.t + 1 == d.t_end);
-    d.ran_prev = d.active;
-    if (d.active) {
-      const uint64_t t0 = d.t - 1;
-      for (int k = 0; k < 32; k++) {
-        const BatchCosDev c = cos_tab[32 * (int64_t)l + k];
-        double v = 1.0;
-        if (c.kind == kCosine) {
-          const double w = 2.0 * kPi / c.period;
-          const double target = c.mean + c.amp * cos(w * (double)t0 + c.phase);
-          if (t0 >= c.warmup) v = target;
-          else {
-            const double fac = (double)t0 / (double)c.warmup;
-            v = fac * target + (1. - fac) * c.min_density;
-          }
-        }
-        dens[32 * (int64_t)l + k] = v;
+  const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+  for (int l = threadIdx.x >> 5; l < n_lat; l += warps) {
+    unsigned long long t = 0;
+    int active = 0;
+    if (lane == 0) {
+      BatchLatDev d = lat[l];
+      if (d.ran_prev) d.t++;
+      d.active = d.t < d.t_end;
+      d.macro = d.active && (d.t + 1 == d.t_end);
+      d.ran_prev = d.active;
+      lat[l] = d;
+      t = d.t;
+      active = d.active;
+      if (d.macro) macro_list[atomicAdd(&listed, 1)] = l;
+    }
+    t = __shfl_sync(0xffffffffu, t, 0);
+    active = __shfl_sync(0xffffffffu, active, 0);
+    if (!active) continue;
+    const uint64_t t0 = t - 1;
+    const BatchCosDev c = cos_tab[32 * (int64_t)l + lane];
+    double v = 1.0;
+    if (c.kind == kCosine) {
+      const double w = 2.0 * kPi / c.period;
+      const double target = c.mean + c.amp * cos(w * (double)t0 + c.phase);
+      if (t0 >= c.warmup) v = target;
+      else {
+        const double fac = (double)t0 / (double)c.warmup;
+        v = fac * target + (1. - fac) * c.min_density;
       }
     }
-    if (d.macro) macro_list[atomicAdd(&listed, 1)] = l;
-    lat[l] = d;
+    dens[32 * (int64_t)l + lane] = v;
   }
   __syncthreads();
   if (threadIdx.x == 0) *macro_count = listed;
@@ -187,9 +358,14 @@ void launch_fill_shift(void* out, int64_t np, int64_t base, int64_t n, const flo
 
 void launch_batch_begin(void* lat, const void* cos_tab, double* dens, int* macro_list, int* macro_count, int n_lat,
                         void* stream) {
-  if (n_lat > 0)
-    k_batch_begin<<<1, 1024, 0, (cudaStream_t)stream>>>(static_cast<BatchLatDev*>(lat), static_cast<const BatchCosDev*>(cos_tab),
-                                                        dens, macro_list, macro_count, n_lat);
+  k_batch_begin<<<1, 1024, 0, (cudaStream_t)stream>>>(static_cast<BatchLatDev*>(lat), static_cast<const BatchCosDev*>(cos_tab),
+                                                      dens, macro_list, macro_count, n_lat);
+}
+
+void launch_batch_ghosts(const BatchArgs& b, int precision, int grid, void* stream) {
+  if (b.iol_count <= 0) return;
+  if (precision == HB_STORE_FP16) k_batch_ghosts<__half><<<grid, 128, 0, (cudaStream_t)stream>>>(b);
+  else k_batch_ghosts<float><<<grid, 128, 0, (cudaStream_t)stream>>>(b);
 }
 
 void launch_batch_macro(const BatchArgs& b, int precision, int grid, void* stream) {
@@ -204,35 +380,26 @@ void launch_fill_ghost(float* ghost, int64_t pitch, int64_t base, int64_t n, con
   if (n > 0) k_fill_ghost<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(ghost, pitch, base, n, r);
 }
 
-void launch_batch_step(const BatchArgs& b, int precision, int spt, int bulk_block, int bulk_grid, int gen_grid,
-                       void* bulk_stream, void* gen_stream) {
-  cudaStream_t sb = (cudaStream_t)bulk_stream, sg = (cudaStream_t)gen_stream;
-  if (b.gen_tiles > 0) {
-    if (precision == HB_STORE_FP16) k_batch_general<__half><<<gen_grid, 128, 0, sg>>>(b);
-    else k_batch_general<float><<<gen_grid, 128, 0, sg>>>(b);
-  }
-  if (b.bulk_tiles > 0) {
-    if (precision == HB_STORE_FP16) {
-      if (spt == 2) k_batch_bulk<__half, 2><<<bulk_grid, bulk_block, 0, sb>>>(b);
-      else k_batch_bulk<__half, 1><<<bulk_grid, bulk_block, 0, sb>>>(b);
-    } else {
-      if (spt == 2) k_batch_bulk<float, 2><<<bulk_grid, bulk_block, 0, sb>>>(b);
-      else k_batch_bulk<float, 1><<<bulk_grid, bulk_block, 0, sb>>>(b);
-    }
+void launch_batch_step(const BatchArgs& b, int precision, int spt, int block, int grid, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((int64_t)b.gen_tiles + b.bulk_tiles <= 0) return;
+  if (precision == HB_STORE_FP16) {
+    if (spt == 2) k_batch_step<__half, 2><<<grid, block, 0, st>>>(b);
+    else k_batch_step<__half, 1><<<grid, block, 0, st>>>(b);
+  } else {
+    if (spt == 2) k_batch_step<float, 2><<<grid, block, 0, st>>>(b);
+    else k_batch_step<float, 1><<<grid, block, 0, st>>>(b);
   }
 }
 
-int batch_occupancy(int precision, int spt, int bulk_block, int* bulk_blocks_per_sm, int* gen_blocks_per_sm) {
+int batch_occupancy(int precision, int spt, int block, int* blocks_per_sm) {
   cudaError_t e;
-  if (precision == HB_STORE_FP16) {
-    e = spt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(bulk_blocks_per_sm, k_batch_bulk<__half, 2>, bulk_block, 0)
-                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(bulk_blocks_per_sm, k_batch_bulk<__half, 1>, bulk_block, 0);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(gen_blocks_per_sm, k_batch_general<__half>, 128, 0);
-  } else {
-    e = spt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(bulk_blocks_per_sm, k_batch_bulk<float, 2>, bulk_block, 0)
-                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(bulk_blocks_per_sm, k_batch_bulk<float, 1>, bulk_block, 0);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(gen_blocks_per_sm, k_batch_general<float>, 128, 0);
-  }
+  if (precision == HB_STORE_FP16)
+    e = spt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_batch_step<__half, 2>, block, 0)
+                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_batch_step<__half, 1>, block, 0);
+  else
+    e = spt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_batch_step<float, 2>, block, 0)
+                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_batch_step<float, 1>, block, 0);
   return e == cudaSuccess ? 0 : -1;
 }
 

@@ -218,12 +218,14 @@ __device__ __forceinline__ void gather_any_m(const StepArgs& a, const MixArgs& m
   else gather_general_m<S, WALL>(a, m, -r - 1, s, g);
 }
 
-__device__ __forceinline__ void flag_unstable_m(const StepArgs& a, const float* g) {
+__device__ __forceinline__ void flag_unstable_status(const float* g, int* status) {
   bool bad = false;
 #pragma unroll
   for (int i = 0; i < Q; i++) bad |= !(wf(i) + g[i] > 0.0f);
-  if (bad) atomicOr(a.status, kStatusUnstable);
+  if (bad) atomicOr(status, kStatusUnstable);
 }
+
+__device__ __forceinline__ void flag_unstable_m(const StepArgs& a, const float* g) { flag_unstable_status(g, a.status); }
 
 // Collision and store of plain bulk site s from its pre-collision g.
 template <class S, int K, bool MACRO>
