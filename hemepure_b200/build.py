@@ -27,7 +27,7 @@ CU_SOURCES = {
     "kernels_batch.cu": [],
 }
 CPP_SOURCES = ["xml.cpp", "config.cpp", "layout.cpp", "solver.cpp", "extraction.cpp", "batch.cpp", "capi.cpp"]
-HEADERS = ["hb_common.h", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h", "mixed_site.cuh", "batch.h", "batch_dev.h"]
+HEADERS = ["hb_common.h", "f64_site.cuh", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h", "mixed_site.cuh", "batch.h", "batch_dev.h"]
 
 
 def _deps_mtime() -> float:

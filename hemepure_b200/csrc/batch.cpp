@@ -72,7 +72,7 @@ int64_t Batch::bytes_for(int64_t site_capacity, int64_t general_capacity, int ma
   const int64_t elem = precision == HB_STORE_FP16 ? 2 : 4;
   const int64_t runs = std::max<int64_t>(1024, site_capacity / 4);
   const int64_t g = std::max<int64_t>(64, general_capacity);
-  return 2 * 19 * np * elem + 2 * 18 * g * 4 + 5 * g * 4 + np * 4 + runs * 20 * 4 + g * (4 * 8 + 18 * 8 + 3 * 8) +
+  return 2 * 19 * np * elem + 2 * 18 * g * 4 + 4 * g * 4 + 2 * g * 5 + np * 4 + runs * 20 * 4 + g * (4 * 8 + 18 * 8 + 3 * 8) +
          np * 5 * 8 + (int64_t)max_lattices * (sizeof(BatchLatDev) + 32 * (sizeof(BatchCosDev) + sizeof(IoletDev) + 8) + 4);
 }
 
@@ -89,7 +89,7 @@ Batch::Batch(int64_t site_capacity, int64_t general_capacity, int max_lattices, 
   run_cap_ = std::max<int64_t>(1024, site_capacity / 4);
   sites_.reset(np_);
   gens_.reset(cap_gen_);
-  iols_.reset(cap_gen_);
+  iols_.reset(2 * cap_gen_);
   runs_.reset(run_cap_);
   for (int s = max_lat_ - 1; s >= 0; s--) free_slots_.push_back(s);
   check(cudaSetDevice(device_), "cudaSetDevice");
@@ -128,7 +128,8 @@ Batch::Batch(int64_t site_capacity, int64_t general_capacity, int max_lattices, 
   alloc(macro_list_, (size_t)max_lat_ * sizeof(int), 0);
   alloc(macro_count_, sizeof(int), 0);
   alloc(io_moments_, (size_t)4 * cap_gen_ * sizeof(float), 0);
-  alloc(iol_list_, (size_t)cap_gen_ * sizeof(int), 0xFF);
+  alloc(iol_list_, (size_t)2 * cap_gen_ * sizeof(int), 0xFF);
+  alloc(iol_link_, (size_t)2 * cap_gen_, 0);
   alloc(rho_, (size_t)np_ * sizeof(double), 0);
   alloc(u_, (size_t)3 * np_ * sizeof(double), 0);
   alloc(wss_, (size_t)np_ * sizeof(double), 0);
@@ -213,9 +214,15 @@ void Batch::write_member_tables(const BatchMember& m) {
     put_rows(g_nrm_, cap_gen_, m.gen_base, L.g_nrm.data(), G, 3, stream_);
     put_rows(g_xyz_, cap_gen_, m.gen_base, L.g_xyz.data(), G, 3, stream_);
     std::vector<int> iol;
+    std::vector<uint8_t> link;
     for (int g = 0; g < G; g++)
-      if (L.g_iolet[g]) iol.push_back(g + (int)m.gen_base);
+      for (int d = 1; d < Q; d++)
+        if ((L.g_iolet[g] >> (d - 1)) & 1u) {
+          iol.push_back(g + (int)m.gen_base);
+          link.push_back((uint8_t)d);
+        }
     put(iol_list_, m.iol_base, iol.data(), (int64_t)iol.size(), stream_);
+    put(iol_link_, m.iol_base, link.data(), (int64_t)link.size(), stream_);
   }
 }
 
@@ -264,7 +271,7 @@ int Batch::add(PreparedLattice& prep) {
   const int64_t run_base = site_base < 0 ? -1 : runs_.take(prep.L.runs);
   const int64_t gen_base = run_base < 0 ? -1 : gens_.take(std::max(1, prep.L.G));
   int64_t iol_len = 0;
-  for (int g = 0; g < prep.L.G; g++) iol_len += prep.L.g_iolet[g] ? 1 : 0;
+  for (int g = 0; g < prep.L.G; g++) iol_len += __builtin_popcount(prep.L.g_iolet[g]);
   const int64_t iol_base = gen_base < 0 ? -1 : iols_.take(std::max<int64_t>(1, iol_len));
   if (site_base < 0 || run_base < 0 || gen_base < 0 || iol_base < 0) {
     if (site_base >= 0) sites_.give(site_base, site_len);
@@ -390,7 +397,7 @@ void Batch::capture(int k) {
   const int grid = std::max(1, std::min(bulk_tiles + gen_tiles, sm_count_ * std::max(1, per_sm)));
   const int macro_grid = 2 * sm_count_;
   const int64_t iols_hw = iols_.high_water();
-  const int ghost_grid = std::max(1, std::min((int)((iols_hw + 127) / 128), 4 * sm_count_));
+  const int ghost_grid = std::max(1, std::min((int)((iols_hw + 127) / 128), 8 * sm_count_));
   int n_lat = 0;
   for (auto& kv : members_) n_lat = std::max(n_lat, kv.first + 1);
 
@@ -434,6 +441,7 @@ void Batch::capture(int k) {
     b.macro_count = macro_count_.as<int>();
     b.io_moments = io_moments_.as<float>();
     b.iol_list = iol_list_.as<int>();
+    b.iol_link = iol_link_.as<uint8_t>();
     b.iol_count = (int)iols_hw;
     b.n_lat = n_lat;
     b.bulk_tiles = bulk_tiles;

@@ -55,7 +55,7 @@ struct BatchMember {
   int kernel = 0, wall = 0;
   int64_t site_base = 0, site_len = 0;
   int64_t run_base = 0, gen_base = 0;
-  int64_t iol_base = 0, iol_len = 0;  // entries of the iolet-record list
+  int64_t iol_base = 0, iol_len = 0;  // entries of the iolet-link lists
   int buffer_at_admission = 0;
   uint64_t steps = 0, t_first = 1;
   bool finished = false;
@@ -109,7 +109,7 @@ class Batch {
   DeviceBuffer f_[2], ghost_[2];
   DeviceBuffer meta_, run_off_;
   DeviceBuffer g_site_, g_run_, g_wall_, g_iolet_, g_src_, g_q_, g_nrm_, g_io_, g_cpl_, g_xyz_, g_lat_;
-  DeviceBuffer lat_, cos_, iolets_, dens_, lat_status_, macro_list_, macro_count_, io_moments_, iol_list_, rho_, u_, wss_;
+  DeviceBuffer lat_, cos_, iolets_, dens_, lat_status_, macro_list_, macro_count_, io_moments_, iol_list_, iol_link_, rho_, u_, wss_;
   int cur_ = 0;
   int spt_ = 2, bulk_block_ = 256;
   int sm_count_ = 148;

@@ -45,7 +45,8 @@ struct BatchArgs {
   int n_lat;
   int bulk_tiles;       // tiles of block*spt sites
   int gen_tiles;        // tiles of block boundary records
-  const int* iol_list;  // boundary records with iolet links (-1: free entry)
+  const int* iol_list;  // record of each iolet link (-1: free entry)
+  const uint8_t* iol_link;  // the link (1..18)
   int iol_count;        // entries of iol_list in use (high-water mark)
 };
 

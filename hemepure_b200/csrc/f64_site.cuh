@@ -1,0 +1,414 @@
+// f64_site.cuh -- per-site device routines of the FP64 collide-and-stream step
+// (kernels_f64.cu).  Every translation unit that includes it is compiled with
+// -fmad=false: each product and sum is rounded separately, in the association
+// order of the reference's SSE3 build.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device.h"
+#include "hb_common.h"
+
+namespace hb {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Lattice maths in the reference's SSE3 order (src/lb/lattices/Lattice.h:51-110, 374-448).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void moments(const double* f, double& rho, double& mx, double& my, double& mz) {
+  double dl = 0.0, dh = f[18];
+  double xl = 0.0, xh = (double)cx(18) * f[18];
+  double yl = 0.0, yh = (double)cy(18) * f[18];
+  double zl = 0.0, zh = (double)cz(18) * f[18];
+#pragma unroll
+  for (int d = 0; d < 18; d += 2) {
+    dl = dl + f[d];
+    dh = dh + f[d + 1];
+    xl = xl + (double)cx(d) * f[d];
+    xh = xh + (double)cx(d + 1) * f[d + 1];
+    yl = yl + (double)cy(d) * f[d];
+    yh = yh + (double)cy(d + 1) * f[d + 1];
+    zl = zl + (double)cz(d) * f[d];
+    zh = zh + (double)cz(d + 1) * f[d + 1];
+  }
+  rho = dl + dh;
+  mx = xl + xh;
+  my = yl + yh;
+  mz = zl + zh;
+}
+
+struct FeqConst {
+  double rho, mx, my, mz, t1, nh;
+  __device__ __forceinline__ FeqConst(double r, double x, double y, double z) : rho(r), mx(x), my(y), mz(z) {
+    const double th = (3. / 2.) * (mx * mx + my * my + mz * mz);
+    const double d1 = 1. / rho;
+    nh = (9. / 2.) * d1;
+    t1 = rho - th * d1;
+  }
+  __device__ __forceinline__ double operator()(int i) const {
+    const double mde = (double)cx(i) * mx + (double)cy(i) * my + (double)cz(i) * mz;
+    return weight(i) * ((t1 + nh * (mde * mde)) + 3. * mde);
+  }
+};
+
+// Relaxation time of the LES kernel (LBGKLESSpongeLayer::CalculateTau and
+// compute_tau_smagorinsky, src/lb/kernels/LBGKLESSpongeLayer.h:122-182).
+__device__ __forceinline__ double les_tau(const StepArgs& a, const double* fneq, double vt) {
+  const double tau0 = a.tau;
+  double q12 = 0.0;
+#pragma unroll
+  for (int p = 0; p < 3; p++)
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      double qij = 0.0;
+#pragma unroll
+      for (int v = 0; v < Q; v++) qij += (double)(cc(p, v) * cc(r, v)) * fneq[v];
+      q12 += qij * qij;
+    }
+  q12 = sqrt(q12);
+  constexpr double kSmag = 18.0 * 1.4142135623730950488016887242097 * 1.0 * 0.1 * 0.1;
+  const double tau_les = 1. / 2. * (tau0 + sqrt((tau0 * 1.0 * 1.0) * (tau0 * 1.0 * 1.0) + kSmag * q12) / (1.0 * 1.0));
+  if (a.t <= a.lifetime / 2) return (vt == tau0) ? tau_les : vt;
+  if (a.t < a.lifetime) return (tau_les - vt) * 2.0 / (double)a.lifetime * (double)a.t + (2.0 * vt - tau_les);
+  return tau_les;
+}
+
+// Post-collision value of direction i for kernel K (LBGK.h:64-72, TRT.h:80-109).
+template <int K>
+__device__ __forceinline__ double collide_one(const StepArgs& a, const double* f, const double* fneq, double omega_site, int i) {
+  if (K == kTRT) {
+    if (i == 0) return f[0] + (0.5 * a.omega * (fneq[0] + fneq[0])) - (0.5 * a.omega_minus * (fneq[0] - fneq[0]));
+    const int j = inv(i);
+    const int lo = i < j ? i : j, hi = i < j ? j : i;
+    const double sym = 0.5 * a.omega * (fneq[lo] + fneq[hi]);
+    const double asym = 0.5 * a.omega_minus * (fneq[lo] - fneq[hi]);
+    return i == lo ? (f[i] + sym + asym) : (f[i] + sym - asym);
+  }
+  return f[i] + fneq[i] * omega_site;
+}
+
+// Wall-shear-stress magnitude (Lattice::CalculateWallShearStressMagnitude,
+// CalculatePiTensor; src/lb/lattices/Lattice.h:1122-1156, 1353-1383).
+__device__ __forceinline__ double wss_mag(double tau, const double* fpost, const double* f, const double nor[3]) {
+  double pi[3][3];
+#pragma unroll
+  for (int p = 0; p < 3; p++)
+#pragma unroll
+    for (int r = 0; r <= p; r++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int l = 0; l < Q; l++) acc += (fpost[l] - f[l]) * (double)cc(p, l) * (double)cc(r, l);
+      pi[p][r] = acc * -(tau - 0.5);
+    }
+  pi[0][1] = pi[1][0];
+  pi[0][2] = pi[2][0];
+  pi[1][2] = pi[2][1];
+  double sv[3] = {0.0, 0.0, 0.0}, sq = 0.0, ns = 0.0;
+#pragma unroll
+  for (int p = 0; p < 3; p++) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) sv[p] += pi[p][r] * nor[r];
+    sq += sv[p] * sv[p];
+    ns += sv[p] * nor[p];
+  }
+  return sqrt(sq - ns * ns);
+}
+
+// InOutLetParabolicVelocity::GetVelocity (src/lb/iolets/InOutLetParabolicVelocity.cc:30-58).
+__device__ __forceinline__ bool parabolic(const IoletDev& I, const double x[3], uint64_t t, double v[3]) {
+  const double dx = x[0] - I.pos[0], dy = x[1] - I.pos[1], dz = x[2] - I.pos[2];
+  const double z = dx * I.nrm[0] + dy * I.nrm[1] + dz * I.nrm[2];
+  const double rsq = (dx * dx + dy * dy + dz * dz) - z * z;
+  const double r2a2 = rsq / (I.radius * I.radius);
+  double mx = I.max_speed;
+  if (t < I.warmup) mx *= (double)t / (double)I.warmup;
+  const double s = mx * (1. - r2a2);
+  v[0] = I.nrm[0] * s;
+  v[1] = I.nrm[1] * s;
+  v[2] = I.nrm[2] * s;
+  return !(r2a2 > 1.0);
+}
+
+__device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
+
+// Pre-collision f of a plain bulk site.
+__device__ __forceinline__ void load_run_offsets(const StepArgs& a, int r, int* off);
+
+__device__ __forceinline__ void gather_bulk(const StepArgs& a, int s, int r, double* f) {
+  int off[20];
+  load_run_offsets(a, r, off);
+  f[0] = ld(a.fin + s);
+#pragma unroll
+  for (int i = 1; i < Q; i++) f[i] = ld(a.fin + (int64_t)i * a.np + (s + off[i]));
+}
+
+// Pre-collision f of general site g (rules above).
+__device__ __forceinline__ void load_run_offsets(const StepArgs& a, int r, int* off) {
+  const int4* o4 = reinterpret_cast<const int4*>(a.run_off) + 5 * r;
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    const int4 v = __ldg(o4 + k);
+    off[4 * k] = v.x;
+    off[4 * k + 1] = v.y;
+    off[4 * k + 2] = v.z;
+    off[4 * k + 3] = v.w;
+  }
+}
+
+template <int WALL>
+__device__ __forceinline__ void gather_general(const StepArgs& a, int g, int s, double* f) {
+  const GeneralDev& G = a.gen;
+  const uint32_t wm = __ldg(G.wall + g), im = __ldg(G.iolet + g);
+  const int run = __ldg(G.run + g);
+  int off[20];
+  if (run >= 0) load_run_offsets(a, run, off);
+  f[0] = ld(a.fin + s);
+#pragma unroll
+  for (int i = 1; i < Q; i++) {
+    const int d = inv(i);
+    const bool bw = (wm >> (d - 1)) & 1u, bi = (im >> (d - 1)) & 1u;
+    if (bi) {
+      f[i] = ld(a.gin + (int64_t)(d - 1) * G.G + g);
+    } else if (bw) {
+      if (WALL == kBFL) {
+        // The cut distance and both values are loaded before the rule is
+        // chosen, so no load waits on another.
+        const bool wi = (wm >> (i - 1)) & 1u;
+        const double fd = ld(a.fin + (int64_t)d * a.np + s);
+        if (wi) {
+          f[i] = fd;
+        } else {
+          const double q = (double)__ldg(G.q + (int64_t)(d - 1) * G.G + g);
+          const double fi = ld(a.fin + (int64_t)i * a.np + s);
+          f[i] = q < 0.5 ? fd : (fd + (2.0 * q - 1) * fi) / (2.0 * q);
+        }
+      } else {
+        f[i] = ld(a.fin + (int64_t)d * a.np + s);
+      }
+    } else {
+      const int src = run >= 0 ? s + off[i] : __ldg(G.src + (int64_t)(i - 1) * G.G + g);
+      f[i] = ld(a.fin + (int64_t)i * a.np + src);
+    }
+  }
+  if (WALL == kBFL && wm) {
+#pragma unroll
+    for (int d = 1; d < Q; d++) {
+      const int i = inv(d);
+      if (((wm >> (d - 1)) & 1u) && !((wm >> (i - 1)) & 1u)) {
+        const double q = (double)__ldg(G.q + (int64_t)(d - 1) * G.G + g);
+        if (q < 0.5) f[i] = 2.0 * q * f[i] + (1.0 - 2.0 * q) * f[d];
+      }
+    }
+  }
+}
+
+// Pre-collision f of any site (GZS neighbours, materialisation).
+template <int WALL, bool GATHER>
+__device__ __forceinline__ void gather_any(const StepArgs& a, int s, double* f) {
+  if (!GATHER) {
+#pragma unroll
+    for (int i = 0; i < Q; i++) f[i] = ld(a.fin + (int64_t)i * a.np + s);
+    return;
+  }
+  const int r = __ldg(a.meta + s);
+  if (r >= 0) gather_bulk(a, s, r, f);
+  else gather_general<WALL>(a, -r - 1, s, f);
+}
+
+__device__ __forceinline__ void flag_unstable(const StepArgs& a, const double* f) {
+  bool bad = false;
+#pragma unroll
+  for (int i = 0; i < Q; i++) bad |= !(f[i] > 0.0);
+  if (bad) atomicOr(a.status, kStatusUnstable);
+}
+
+// ---------------------------------------------------------------------------
+// Per-site steps
+// ---------------------------------------------------------------------------
+
+// One plain bulk site s of run r.
+template <int K, bool GATHER, bool MACRO>
+__device__ __forceinline__ void bulk_site_f64(const StepArgs& a, int s, int r) {
+  double f[Q];
+  if (GATHER) gather_bulk(a, s, r, f);
+  else {
+#pragma unroll
+    for (int i = 0; i < Q; i++) f[i] = ld(a.fin + (int64_t)i * a.np + s);
+  }
+  flag_unstable(a, f);
+  double rho, mx, my, mz;
+  moments(f, rho, mx, my, mz);
+  const FeqConst feq(rho, mx, my, mz);
+  double fneq[Q];
+#pragma unroll
+  for (int i = 0; i < Q; i++) fneq[i] = f[i] - feq(i);
+  double om = a.omega, tau = a.tau;
+  if (K == kLES) {
+    tau = les_tau(a, fneq, __ldg(a.vtau + s));
+    om = -1.0 / tau;
+  }
+#pragma unroll
+  for (int i = 0; i < Q; i++) a.fout[(int64_t)i * a.np + s] = collide_one<K>(a, f, fneq, om, i);
+  if (MACRO) {
+    a.rho[s] = rho;
+    a.u[s] = mx / rho;
+    a.u[a.np + s] = my / rho;
+    a.u[2 * a.np + s] = mz / rho;
+    a.wss[s] = kNoValue;
+  }
+}
+
+// One general (boundary or irregular) site record g.
+template <int K, int WALL, bool GATHER, bool MACRO>
+__device__ __forceinline__ void general_site_f64(const StepArgs& a, int g) {
+  const GeneralDev& G = a.gen;
+  const int s = __ldg(G.site + g);
+  const uint32_t wm = __ldg(G.wall + g), im = __ldg(G.iolet + g);
+  double f[Q];
+  if (GATHER) gather_general<WALL>(a, g, s, f);
+  else {
+#pragma unroll
+    for (int i = 0; i < Q; i++) f[i] = ld(a.fin + (int64_t)i * a.np + s);
+  }
+  flag_unstable(a, f);
+  double rho, mx, my, mz;
+  moments(f, rho, mx, my, mz);
+  const double ux = mx / rho, uy = my / rho, uz = mz / rho;
+  const FeqConst feq(rho, mx, my, mz);
+  double fneq[Q];
+#pragma unroll
+  for (int i = 0; i < Q; i++) fneq[i] = f[i] - feq(i);
+  double om = a.omega, tau = a.tau;
+  if (K == kLES) {
+    tau = les_tau(a, fneq, __ldg(a.vtau + s));
+    om = -1.0 / tau;
+  }
+  double fp[Q];
+#pragma unroll
+  for (int i = 0; i < Q; i++) fp[i] = collide_one<K>(a, f, fneq, om, i);
+  double out[Q];
+#pragma unroll
+  for (int i = 0; i < Q; i++) out[i] = fp[i];
+
+  int io = -1;
+  if (im) io = __ldg(G.io + g);
+  if (im) {
+    const IoletDev& I = a.iolets[io];
+    const int kind = I.kind;
+    double pos[3] = {(double)__ldg(G.xyz + g), (double)__ldg(G.xyz + G.G + g), (double)__ldg(G.xyz + 2 * G.G + g)};
+#pragma unroll
+    for (int d = 1; d < Q; d++) {
+      if (!((im >> (d - 1)) & 1u)) continue;
+      if (kind == kParabolic) {
+        // LaddIoletDelegate::StreamLink (src/lb/streamers/LaddIoletDelegate.h:37-86).
+        double hw[3] = {pos[0], pos[1], pos[2]};
+        hw[0] += 0.5 * cx(d);
+        hw[1] += 0.5 * cy(d);
+        hw[2] += 0.5 * cz(d);
+        double w[3];
+        if (!parabolic(I, hw, (uint64_t)(unsigned int)a.t, w)) {
+          atomicOr(a.status, kStatusIoletRadius);
+          w[0] = w[1] = w[2] = 0.0;
+        }
+        w[0] *= rho;
+        w[1] *= rho;
+        w[2] *= rho;
+        const double corr = 2. * weight(d) * (w[0] * cx(d) + w[1] * cy(d) + w[2] * cz(d)) / kCs2;
+        a.gout[(int64_t)(d - 1) * G.G + g] = fp[d] - corr;
+      } else {
+        // NashZerothOrderPressureDelegate::StreamLink (src/lb/streamers/NashZerothOrderPressureDelegate.h:36-76).
+        const double rb = a.dens_row[io];
+        const double nx = I.nrm_f[0], ny = I.nrm_f[1], nz = I.nrm_f[2];
+        const double comp = (mx / rho) * nx + (my / rho) * ny + (mz / rho) * nz;
+        const FeqConst gq(rb, nx * comp * rb, ny * comp * rb, nz * comp * rb);
+        a.gout[(int64_t)(d - 1) * G.G + g] = gq(inv(d));
+      }
+    }
+  }
+  if (WALL == kGZS && wm) {
+    // GuoZhengShiDelegate::StreamLink (src/lb/streamers/GuoZhengShiDelegate.h:127-293).
+#pragma unroll
+    for (int d = 1; d < Q; d++) {
+      if (!((wm >> (d - 1)) & 1u)) continue;
+      const int i = inv(d);
+      const double q = (double)__ldg(G.q + (int64_t)(d - 1) * G.G + g);
+      const double fac = 1. - 1. / q;
+      double mw0 = mx * fac, mw1 = my * fac, mw2 = mz * fac;
+      double fnw_i = fneq[i], fnw_d = fneq[d];
+      bool sbb = false;
+      if (q < 0.75) {
+        if ((im >> (i - 1)) & 1u) {
+          const IoletDev& I = a.iolets[io];
+          if (I.kind != kParabolic) {
+            sbb = true;
+          } else {
+            double np3[3] = {(double)__ldg(G.xyz + g) + cx(i), (double)__ldg(G.xyz + G.G + g) + cy(i),
+                             (double)__ldg(G.xyz + 2 * G.G + g) + cz(i)};
+            double nv[3];
+            if (!parabolic(I, np3, (uint64_t)(unsigned int)a.t, nv)) {
+              atomicOr(a.status, kStatusIoletRadius);
+              nv[0] = nv[1] = nv[2] = 0.0;
+            }
+            mw0 = q * mw0 + (1. - q) * rho * (nv[0] * (q - 1) / (q + 1));
+            mw1 = q * mw1 + (1. - q) * rho * (nv[1] * (q - 1) / (q + 1));
+            mw2 = q * mw2 + (1. - q) * rho * (nv[2] * (q - 1) / (q + 1));
+          }
+        } else if ((wm >> (i - 1)) & 1u) {
+          sbb = true;
+        } else {
+          const int grun = __ldg(G.run + g);
+          const int nb = grun >= 0 ? s + __ldg(a.run_off + 20 * grun + d) : __ldg(G.src + (int64_t)(d - 1) * G.G + g);
+          double fn[Q];
+          gather_any<WALL, GATHER>(a, nb, fn);
+          double rn, mnx, mny, mnz;
+          moments(fn, rn, mnx, mny, mnz);
+          const double vn0 = mnx / rn, vn1 = mny / rn, vn2 = mnz / rn;
+          const FeqConst fqn(rn, mnx, mny, mnz);
+          mw0 = q * mw0 + (1. - q) * rho * (vn0 * (q - 1) / (q + 1));
+          mw1 = q * mw1 + (1. - q) * rho * (vn1 * (q - 1) / (q + 1));
+          mw2 = q * mw2 + (1. - q) * rho * (vn2 * (q - 1) / (q + 1));
+          fnw_i = q * fnw_i + (1. - q) * (fn[i] - fqn(i));
+          fnw_d = q * fnw_d + (1. - q) * (fn[d] - fqn(d));
+        }
+      }
+      if (sbb) continue;  // slot i reads f*_d, already in out[d]
+      const FeqConst fqw(rho, mw0, mw1, mw2);
+      const double fw_i = fqw(i) + fnw_i;
+      double v;
+      if (K == kTRT) {
+        const int lo = i < d ? i : d;
+        const double fn_lo = lo == i ? fnw_i : fnw_d, fn_hi = lo == i ? fnw_d : fnw_i;
+        const double sym = 0.5 * a.omega * (fn_lo + fn_hi);
+        const double asym = 0.5 * a.omega_minus * (fn_lo - fn_hi);
+        v = i == lo ? (fw_i + sym + asym) : (fw_i + sym - asym);
+      } else {
+        v = fw_i + fnw_i * om;
+      }
+      out[d] = v;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < Q; i++) a.fout[(int64_t)i * a.np + s] = out[i];
+
+  const int cpl = im ? __ldg(G.cpl + g) : -1;
+  if (cpl >= 0) {
+    const IoletDev& I = a.iolets[io];
+    a.cpl_buf[cpl] = ux * (-I.nrm[0]) + uy * (-I.nrm[1]) + uz * (-I.nrm[2]);
+  }
+  if (MACRO) {
+    a.rho[s] = rho;
+    a.u[s] = ux;
+    a.u[a.np + s] = uy;
+    a.u[2 * a.np + s] = uz;
+    if (wm) {
+      const double nor[3] = {(double)__ldg(G.nrm + g), (double)__ldg(G.nrm + G.G + g), (double)__ldg(G.nrm + 2 * G.G + g)};
+      a.wss[s] = wss_mag(tau, fp, f, nor);
+    } else {
+      a.wss[s] = kNoValue;
+    }
+  }
+}
+
+}  // namespace
+}  // namespace hb

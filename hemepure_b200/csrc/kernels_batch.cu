@@ -80,8 +80,7 @@ __device__ __forceinline__ void gather_general_rt(const StepArgs& a, const MixAr
       if (bfl && !wi) {
         const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
         const float fi = ldg_s<S>(m, (int64_t)i * a.np + s);
-        if (q < 0.5f) g[i] = fd;
-        else g[i] = (fd + (2.0f * q - 1.0f) * fi) / (2.0f * q);
+        g[i] = q < 0.5f ? fd : (fd + (2.0f * q - 1.0f) * fi) / (2.0f * q);
       } else {
         g[i] = fd;
       }
@@ -207,49 +206,47 @@ __global__ void __launch_bounds__(256, SPT == 1 ? 4 : 3) k_batch_step(const Batc
 // Iolet ghosts of the boundary records stepped by k_batch_step: the Nash
 // zeroth-order pressure and Ladd velocity rules of general_site_m, from the
 // record's post-collision values (in fout) and its pre-collision density and
-// velocity (io_moments).
+// velocity (io_moments).  One thread per iolet link (record and link from two
+// parallel lists), so the FP64 profile arithmetic of a record's links runs in
+// parallel.
 template <class S>
 __global__ void __launch_bounds__(128) k_batch_ghosts(const BatchArgs b) {
   const GeneralDev& G = b.base.gen;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < b.iol_count; k += gridDim.x * blockDim.x) {
     const int gi = __ldg(b.iol_list + k);
     if (gi < 0) continue;
-    const uint32_t im = __ldg(G.iolet + gi);
+    const int link = b.iol_link[k];
     const int l = __ldg(b.g_lat + gi);
     if (l < 0) continue;
     const BatchLatDev& d = b.lat[l];
     if (!d.active || d.macro) continue;
-    const int s = __ldg(G.site + gi);
-    const float rho = b.io_moments[gi], ux = b.io_moments[G.G + gi], uy = b.io_moments[2 * (int64_t)G.G + gi],
-                uz = b.io_moments[3 * (int64_t)G.G + gi];
     const int io = __ldg(G.io + gi);
     const IoletDev& I = b.base.iolets[32 * (int64_t)l + io];
-    const double pos[3] = {(double)__ldg(G.xyz + gi), (double)__ldg(G.xyz + G.G + gi), (double)__ldg(G.xyz + 2 * G.G + gi)};
-    const uint64_t t = (uint64_t)(unsigned int)d.t;
-#pragma unroll
-    for (int k = 1; k < Q; k++) {
-      if (!((im >> (k - 1)) & 1u)) continue;
-      float v;
-      if (I.kind == kParabolic) {
-        const double hw[3] = {pos[0] + 0.5 * cx(k), pos[1] + 0.5 * cy(k), pos[2] + 0.5 * cz(k)};
-        float w[3];
-        if (!parabolic_f(I, hw, t, w)) {
-          atomicOr(b.lat_status + l, kStatusIoletRadius);
-          w[0] = w[1] = w[2] = 0.0f;
-        }
-        const float corr = 2.0f * wf(k) * rho * (w[0] * cx(k) + w[1] * cy(k) + w[2] * cz(k)) * 3.0f;
-        v = Store<S>::load(b.fout, (int64_t)k * b.base.np + s) - corr;
-      } else {
-        const double rb = b.dens[32 * (int64_t)l + io];
-        const float drb = (float)(rb - 1.0);
-        const float rbf = (float)rb;
-        const float nx = (float)I.nrm_f[0], ny = (float)I.nrm_f[1], nz = (float)I.nrm_f[2];
-        const float comp = ux * nx + uy * ny + uz * nz;
-        const GeqF gq(drb, nx * comp * rbf, ny * comp * rbf, nz * comp * rbf);
-        v = gq(inv(k));
+    const float rho = b.io_moments[gi];
+    float v;
+    if (I.kind == kParabolic) {
+      const int s = __ldg(G.site + gi);
+      const double hw[3] = {(double)__ldg(G.xyz + gi) + 0.5 * cx(link), (double)__ldg(G.xyz + G.G + gi) + 0.5 * cy(link),
+                            (double)__ldg(G.xyz + 2 * G.G + gi) + 0.5 * cz(link)};
+      float w[3];
+      if (!parabolic_f(I, hw, (uint64_t)(unsigned int)d.t, w)) {
+        atomicOr(b.lat_status + l, kStatusIoletRadius);
+        w[0] = w[1] = w[2] = 0.0f;
       }
-      b.gout[(int64_t)(k - 1) * G.G + gi] = v;
+      const float corr = 2.0f * wf(link) * rho * (w[0] * cx(link) + w[1] * cy(link) + w[2] * cz(link)) * 3.0f;
+      v = Store<S>::load(b.fout, (int64_t)link * b.base.np + s) - corr;
+    } else {
+      const float ux = b.io_moments[G.G + gi], uy = b.io_moments[2 * (int64_t)G.G + gi],
+                  uz = b.io_moments[3 * (int64_t)G.G + gi];
+      const double rb = b.dens[32 * (int64_t)l + io];
+      const float drb = (float)(rb - 1.0);
+      const float rbf = (float)rb;
+      const float nx = (float)I.nrm_f[0], ny = (float)I.nrm_f[1], nz = (float)I.nrm_f[2];
+      const float comp = ux * nx + uy * ny + uz * nz;
+      const GeqF gq(drb, nx * comp * rbf, ny * comp * rbf, nz * comp * rbf);
+      v = gq(inv(link));
     }
+    b.gout[(int64_t)(link - 1) * G.G + gi] = v;
   }
 }
 

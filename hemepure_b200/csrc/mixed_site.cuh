@@ -182,10 +182,15 @@ __device__ __forceinline__ void gather_general_m(const StepArgs& a, const MixArg
     } else if (bw) {
       const float fd = ldg_s<S>(m, (int64_t)d * a.np + s);
       if (WALL == kBFL) {
-        const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
+        // The cut distance and both values are loaded before the rule is chosen.
         const bool wi = (wm >> (i - 1)) & 1u;
-        if (wi || q < 0.5f) g[i] = fd;
-        else g[i] = (fd + (2.0f * q - 1.0f) * ldg_s<S>(m, (int64_t)i * a.np + s)) / (2.0f * q);
+        if (wi) {
+          g[i] = fd;
+        } else {
+          const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
+          const float fi = ldg_s<S>(m, (int64_t)i * a.np + s);
+          g[i] = q < 0.5f ? fd : (fd + (2.0f * q - 1.0f) * fi) / (2.0f * q);
+        }
       } else {
         g[i] = fd;
       }

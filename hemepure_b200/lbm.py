@@ -315,7 +315,9 @@ class LBM:
         return float(ms.value), int(n.value)
 
     def profile_steps(self, n: int):
-        """Advance `n` steps timing each launch: (bulk ms, general ms, windkessel ms)."""
+        """Advance 2n steps timing the launches: (step launch ms over the first n
+        steps as `step` runs them, plain-bulk kernel ms and boundary kernel ms
+        over the next n steps run one kernel after the other)."""
         ms = np.zeros(3)
         self._check(library().hb_profile_steps(self._h, int(n), _p(ms)))
         return float(ms[0]), float(ms[1]), float(ms[2])

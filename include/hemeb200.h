@@ -272,9 +272,11 @@ int hb_moment_sums_noalloc(const double* f, int64_t dir_stride, int64_t site_str
 /* Device-time of the last hb_step call's kernels in milliseconds (CUDA events),
  * and the number of kernel launches it made. */
 int hb_last_step_timing(const hb_handle* h, double* ms, int64_t* launches);
-/* Advance `n_steps` steps with CUDA events around every launch (serialises the
- * launches; for measurement only): ms[0] plain-bulk kernel, ms[1] boundary
- * (general-site) kernel, ms[2] Windkessel kernel, summed over the steps. */
+/* Advance 2 x `n_steps` steps with CUDA events around the launches (for
+ * measurement only).  The first n_steps run as hb_step runs them and ms[0]
+ * sums their collide-and-stream launch (one fused kernel, or the bulk and
+ * boundary kernels side by side); the next n_steps run the plain-bulk kernel
+ * and then the boundary kernel, and ms[1] and ms[2] sum those. */
 int hb_profile_steps(hb_handle* h, int64_t n_steps, double ms[3]);
 /* Bytes of device memory held by the handle. */
 int hb_device_bytes(const hb_handle* h, int64_t* bytes);

@@ -114,3 +114,13 @@ def test_batch_preparation_is_host_only(case_dir):
     with pytest.raises(lbm.HemeLBError) as e:
         lbm.PreparedLattice(xml, kernel, wall, 100)     # LBGK+LES is not run batched
     assert e.value.code == -7
+
+
+def test_empty_lattice_is_refused():
+    """A lattice with no sites is an argument error, raised before any device work."""
+    empty = {"coords": np.zeros((0, 3), np.int64), "dims": [1, 1, 1], "wall_mask": np.zeros(0, np.uint32),
+             "iolet_mask": np.zeros(0, np.uint32), "site_type": np.zeros(0, np.int32),
+             "iolet_id": np.zeros(0, np.int32)}
+    with pytest.raises(lbm.HemeLBError) as e:
+        lbm.LBM(lattice=empty, params=lbm.Params())
+    assert e.value.code == -1
