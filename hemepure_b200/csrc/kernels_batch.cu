@@ -140,8 +140,11 @@ __device__ __forceinline__ void batch_general_tile(const BatchArgs& b, const Mix
 
 // A tile of SPT * blockDim sites, plain bulk ones taken.  The run row carries
 // the lattice slot in its spare last entry, so the site's run offsets and its
-// lattice come in one load; all SPT sites of a thread are gathered before any
-// relaxes, so their loads are in flight together.
+// lattice come in one load.  The gather is issued together with the load of
+// the lattice's flags rather than after it: the loads stay inside the lattice's
+// own range, and one that is not stepping (finished, awaiting retirement at the
+// end of the block) only wastes them.  All SPT sites of a thread are gathered
+// before any relaxes, so their loads are in flight together.
 template <class S, int SPT>
 __device__ __forceinline__ void batch_bulk_tile(const BatchArgs& b, const MixArgs& m, int tile) {
   int s[SPT], l[SPT];
@@ -155,11 +158,10 @@ __device__ __forceinline__ void batch_bulk_tile(const BatchArgs& b, const MixArg
     if (r < 0) continue;
     int off[20];
     run_offsets(b.base, r, off);
-    if (!lattice_steps(b, off[19])) continue;
-    l[k] = off[19];
     g[k][0] = ldg_s<S>(m, s[k]);
 #pragma unroll
     for (int i = 1; i < Q; i++) g[k][i] = ldg_s<S>(m, (int64_t)i * b.base.np + (s[k] + off[i]));
+    if (lattice_steps(b, off[19])) l[k] = off[19];
   }
 #pragma unroll
   for (int k = 0; k < SPT; k++) {
