@@ -9,6 +9,7 @@
 #include "batch.h"
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstring>
 
@@ -477,14 +478,26 @@ std::vector<int> Batch::run(int k) {
   cur_ = (cur_ + k) & 1;
   if (k % 2) dirty_ = true;
   std::vector<BatchLatDev> lat(max_lat_);
+  std::vector<int> status(max_lat_);
   check(cudaMemcpy(lat.data(), lat_.p, (size_t)max_lat_ * sizeof(BatchLatDev), cudaMemcpyDeviceToHost), "lattice records");
+  check(cudaMemcpy(status.data(), lat_status_.p, (size_t)max_lat_ * sizeof(int), cudaMemcpyDeviceToHost), "status");
   for (auto& kv : members_) {
     BatchMember& m = *kv.second;
     if (m.finished) continue;
     const BatchLatDev& d = lat[m.slot];
-    if (d.t + (uint64_t)d.ran_prev >= d.t_end) {
+    const uint64_t reached = d.t + (uint64_t)d.ran_prev;
+    if (reached >= d.t_end) {
       m.finished = true;
       done.push_back(m.slot);
+    } else if (status[m.slot]) {
+      // Unstable (or a parabolic point outside its iolet): stop stepping it and
+      // hand it back now; its macroscopic fields are not filled.
+      m.finished = true;
+      done.push_back(m.slot);
+      const uint64_t t_end = reached;
+      check(cudaMemcpy(reinterpret_cast<char*>(lat_.as<BatchLatDev>() + m.slot) + offsetof(BatchLatDev, t_end), &t_end,
+                       sizeof(t_end), cudaMemcpyHostToDevice),
+            "stop member");
     }
   }
   return done;

@@ -72,7 +72,8 @@ class Batch {
   int add(PreparedLattice& prep);
   void remove(int slot);
   // Run `k` steps of every active member (a captured CUDA graph per block
-  // length); returns the slots that finished during the block.
+  // length); returns the slots that finished during the block: reached their
+  // step count, or went unstable (then stopped, their fields not filled).
   std::vector<int> run(int k);
   // Macroscopic fields of a finished member's last step, reference order.
   void get_macro(int slot, double* rho, double* u, double* wss);

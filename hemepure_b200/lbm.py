@@ -459,7 +459,8 @@ class Batch:
         self._check(library().hb_batch_remove(self._b, int(slot)))
 
     def run(self, k: int):
-        """Run k steps; returns the slots that finished in this block."""
+        """Run k steps; returns the slots that finished in this block: reached
+        their step count, or went unstable (check `info`; then no fields)."""
         buf = (C.c_int * self.max_lattices)()
         n = C.c_int()
         self._check(library().hb_batch_run(self._b, int(k), buf, self.max_lattices, C.byref(n)))

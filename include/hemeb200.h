@@ -219,8 +219,10 @@ int hb_batch_prepare_xml(const char* xml_path, int kernel, int wall, uint64_t st
 int hb_batch_prep_sites(const hb_batch_prep* prep, int64_t* sites);
 int hb_batch_add_prepared(hb_batch* b, hb_batch_prep* prep, int* slot);
 int hb_batch_prep_free(hb_batch_prep* prep);
-/* Run a block of k steps; the slots that reached their step count are written
- * to finished[0 .. *n_finished) (at most max_finished). */
+/* Run a block of k steps; the slots that reached their step count, or went
+ * unstable during the block (status bits set; such a member stops stepping and
+ * its macroscopic fields are not filled), are written to
+ * finished[0 .. *n_finished) (at most max_finished). */
 int hb_batch_run(hb_batch* b, int k, int* finished, int max_finished, int* n_finished);
 /* Density [n], velocity [n*3], wall shear stress [n] of a finished member's last step, reference order. */
 int hb_batch_get_macro(hb_batch* b, int slot, double* density, double* velocity, double* wss);
