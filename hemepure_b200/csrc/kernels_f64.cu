@@ -27,6 +27,8 @@
 namespace hb {
 namespace {
 
+constexpr int kGeneralBlocksPerSM = 8;
+
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
@@ -40,8 +42,14 @@ __global__ void __launch_bounds__(256) k_bulk(const StepArgs a) {
   bulk_site_f64<K, GATHER, MACRO>(a, s, r);
 }
 
+// The boundary kernel is latency-bound: with LBGK or TRT, bounce-back or BFL
+// walls and no outputs it is held to 64 registers so that 16 warps per SM hide
+// its dependent loads (it spills a little; LBGK/BFL measured 20% faster than at
+// 94 registers, and the whole step 5% faster).  The LES kernel, GZS walls and
+// output steps, which would spill far more, keep the compiler's allocation.
 template <int K, int WALL, bool GATHER, bool MACRO>
-__global__ void __launch_bounds__(128) k_general(const StepArgs a) {
+__global__ void __launch_bounds__(128, (K != kLES && WALL != kGZS && !MACRO) ? kGeneralBlocksPerSM : 1)
+    k_general(const StepArgs a) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= a.gen.G) return;
   general_site_f64<K, WALL, GATHER, MACRO>(a, g);
