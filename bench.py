@@ -111,6 +111,23 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of the ranks' values (device timings are reported as the
+    slowest rank's); `dist` is torch.distributed or None for one rank."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_mlups(world: int, n_sites: int, steps: int, ms_max: float) -> float:
+    """Whole-job MLUPS of `world` replicas each stepping `n_sites` sites `steps`
+    times, over the slowest rank's device time `ms_max`."""
+    return world * n_sites * steps / (ms_max * 1e-3) / 1e6
+
+
 def make_workload(name: str, out_dir: str):
     from hemepure_b200 import vessels
     xml, gmy, info = vessels.make_case(name, out_dir)
@@ -187,6 +204,8 @@ def main():
     desc, kernel, wall, bytes_per_site = WORKLOADS[args.workload]
     warmup = max(3, args.warmup)
 
+    if args.impl == "reference" and rank != 0:
+        return  # the reference arm runs on rank 0 only; the other ranks exit without work
     case_root = args.case_dir or os.path.join(tempfile.gettempdir(), f"hemeb200_bench_{os.getuid()}")
     case_dir = os.path.join(case_root, f"{args.workload}_rank{rank}")
     xml, info = make_workload(args.workload, case_dir)
@@ -196,8 +215,6 @@ def main():
               % (19 * n_sites * 8 / 1e9), "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
     if args.impl == "reference":
-        if rank != 0:
-            return
         # The reference itself cannot be built here (it needs MPI, Boost and ParMETIS,
         # which are absent); its algorithm runs as the C restatement on all host threads.
         total_budget = 150.0
@@ -247,11 +264,8 @@ def main():
     torch.cuda.synchronize()
     ms, launches = sim.last_step_timing()
     clocks = sampler.stop()
-    if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * n_sites * args.steps / (ms * 1e-3) / 1e6
+    ms = max_over_ranks(ms, dist, f"cuda:{local}")
+    value = replica_mlups(world, n_sites, args.steps, ms)
 
     # Roofline of the dominant kernel (the plain-bulk kernel, three quarters of the
     # step): per-launch CUDA events.  The step's launch pair (bulk and boundary
@@ -287,11 +301,7 @@ def main():
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         sim.step(1)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
     e2e = {"value": world * n_sites * e2e_steps / e2e_s / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": 32 * 8,
            "d2h_bytes_per_step": 4, "steps": e2e_steps,
            "note": "one hb_step(1) call per step: iolet densities up, stability word down, host sync"}
