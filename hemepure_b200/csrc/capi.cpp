@@ -268,6 +268,15 @@ int hb_write_xtr(hb_handle* h, const char* path, const char* fields, const char*
   });
 }
 
+int hb_write_xtr_selected(hb_handle* h, const char* path, const char* fields, const char* offset_path,
+                          const hb_selector* sel) {
+  if (!h || !path || !fields || !sel) return HB_ERR_ARG;
+  return guard(h, [&] {
+    hb::write_xtr(*h->solver, path, fields, offset_path ? offset_path : "", sel);
+    return HB_OK;
+  });
+}
+
 int hb_read_checkpoint(hb_handle* h, const char* path, uint64_t step) {
   if (!h || !path) return HB_ERR_ARG;
   return guard(h, [&] {
@@ -462,6 +471,16 @@ int hb_geometry_site_count(const hb_geometry* g, int64_t* n, int64_t dims[3]) {
   if (dims)
     for (int d = 0; d < 3; d++) dims[d] = g->tables.dims[d];
   return HB_OK;
+}
+
+int hb_geometry_select(const hb_geometry* g, const hb_selector* sel, double voxel_size, const double origin[3],
+                       uint8_t* mask) {
+  if (!g || !sel || !origin || !mask || !(voxel_size > 0)) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    const std::vector<uint8_t> m = hb::select_sites(g->tables, *sel, voxel_size, origin);
+    std::memcpy(mask, m.data(), m.size());
+    return HB_OK;
+  });
 }
 
 int hb_geometry_tables(const hb_geometry* g, int64_t* neighbours, uint32_t* wall_mask, uint32_t* iolet_mask,

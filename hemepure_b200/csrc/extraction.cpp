@@ -18,6 +18,7 @@
 
 #include <sys/stat.h>
 
+#include <cmath>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -121,11 +122,100 @@ std::vector<unsigned char> read_file(const std::string& path) {
   return std::vector<unsigned char>((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
 }
 
+// util::Vector3D<float> arithmetic of the reference's selectors: every operation
+// rounds to float (the host build does not contract products into FMAs).
+struct V3f {
+  float x, y, z;
+};
+V3f sub(V3f a, V3f b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+V3f add(V3f a, V3f b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+V3f mul(V3f a, float k) { return {a.x * k, a.y * k, a.z * k}; }
+V3f div(V3f a, float k) { return {a.x / k, a.y / k, a.z / k}; }
+float dot(V3f a, V3f b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+float mag(V3f a) { return std::sqrt(dot(a, a)); }
+V3f to_f(const double v[3]) { return {(float)v[0], (float)v[1], (float)v[2]}; }
+V3f normalised(V3f v) {  // Vector3D::GetNormalised (util/Vector3D.h:270-292)
+  if (v.x == 0.0f && v.y == 0.0f && v.z == 0.0f) return v;
+  return div(v, mag(v));
+}
+
 }  // namespace
 
-void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv, const std::string& offset_path) {
+std::vector<uint8_t> select_sites(const LatticeTables& t, const hb_selector& sel, double voxel, const double origin[3]) {
+  const int64_t n = t.n;
+  std::vector<uint8_t> mask((size_t)n, 0);
+  if (sel.type < HB_SELECT_WHOLE || sel.type > HB_SELECT_SURFACE_POINT) throw Error{HB_ERR_ARG, "unknown geometry selector"};
+  // Selector state as the reference's constructors hold it: float vectors and radii.
+  const V3f point = to_f(sel.point), point2 = to_f(sel.point2);
+  const V3f normal = normalised(to_f(sel.normal));
+  const float radius = (float)sel.radius;
+  const V3f line = sub(point2, point);
+  const float line_len = mag(line);
+  const float max_surface_dist = (float)std::sqrt(3.0);
+  for (int64_t i = 0; i < n; i++) {
+    const bool wall = t.wall[i] != 0;
+    // Vector3D<float>(location) * voxel + origin, in double, stored as float.
+    const V3f c = {(float)((double)(float)t.coords[3 * i] * voxel + origin[0]),
+                   (float)((double)(float)t.coords[3 * i + 1] * voxel + origin[1]),
+                   (float)((double)(float)t.coords[3 * i + 2] * voxel + origin[2])};
+    bool take = false;
+    switch (sel.type) {
+      case HB_SELECT_WHOLE:
+        take = true;
+        break;
+      case HB_SELECT_PLANE: {
+        const float perp = dot(sub(c, point), normal);
+        if (std::abs(perp) > 0.5 * voxel) break;
+        if (radius <= 0.) {
+          take = true;
+          break;
+        }
+        const float r2 = dot(sub(sub(c, mul(normal, perp)), point), sub(sub(c, mul(normal, perp)), point));
+        take = r2 <= radius * radius;
+        break;
+      }
+      case HB_SELECT_LINE: {
+        const float along = dot(line, sub(c, point)) / line_len;
+        if (along < 0. || along > line_len) break;
+        const V3f d = sub(add(point, div(mul(line, along), line_len)), c);
+        take = dot(d, d) <= 2.0 * 0.5 * 0.5 * voxel * voxel;
+        break;
+      }
+      case HB_SELECT_SPHERE:
+        take = mag(sub(c, point)) <= radius;
+        break;
+      case HB_SELECT_INLET:
+        take = t.stype[i] == 1;
+        break;
+      case HB_SELECT_OUTLET:
+        take = t.stype[i] == 2;
+        break;
+      case HB_SELECT_SURFACE:
+        take = wall;
+        break;
+      case HB_SELECT_SURFACE_WITHIN_SPHERE:
+        take = wall && mag(sub(c, point)) <= radius;
+        break;
+      case HB_SELECT_SURFACE_POINT: {
+        if (!wall) break;
+        const float d = (float)(mag(sub(c, point)) / voxel);
+        take = d <= max_surface_dist;
+        break;
+      }
+    }
+    mask[(size_t)i] = take ? 1 : 0;
+  }
+  return mask;
+}
+
+void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv, const std::string& offset_path,
+               const hb_selector* sel) {
   const std::vector<std::string> fields = split_fields(fields_csv);
   const LatticeTables& t = s.tables();
+  std::vector<uint8_t> take;
+  if (sel) take = select_sites(t, *sel, s.dx(), s.origin());
+  int64_t n_out = 0;
+  for (int64_t i = 0; i < t.n; i++) n_out += (!sel || take[(size_t)i]) ? 1 : 0;
   const int64_t n = t.n;
   if (s.time_step() <= 1) throw Error{HB_ERR_ARG, "no completed time step to write"};
   const uint64_t label = s.time_step() - 1;
@@ -168,7 +258,7 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
     hdr.f64(s.origin()[0]);
     hdr.f64(s.origin()[1]);
     hdr.f64(s.origin()[2]);
-    hdr.u64((uint64_t)n);
+    hdr.u64((uint64_t)n_out);
     hdr.u32((uint32_t)fields.size());
     hdr.u32((uint32_t)fh.b.size());
     hdr.b.insert(hdr.b.end(), fh.b.begin(), fh.b.end());
@@ -176,6 +266,7 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
   XdrOut rec;
   rec.u64(label);
   for (int64_t i = 0; i < n; i++) {
+    if (sel && !take[(size_t)i]) continue;
     rec.u32((uint32_t)t.coords[3 * i]);
     rec.u32((uint32_t)t.coords[3 * i + 1]);
     rec.u32((uint32_t)t.coords[3 * i + 2]);

@@ -4,13 +4,22 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
+
+#include "../../include/hemeb200.h"
 
 namespace hb {
 
 class Solver;
+struct LatticeTables;
 
-// Append one output record for the whole lattice.
-void write_xtr(Solver& s, const std::string& path, const std::string& fields, const std::string& offset_path);
+// Sites an extraction geometry selector takes (src/extraction/*Selector.cc), as
+// a mask over the lattice in contiguous order; voxel size and origin in metres.
+std::vector<uint8_t> select_sites(const LatticeTables& t, const hb_selector& sel, double voxel, const double origin[3]);
+
+// Append one output record for the sites `sel` takes (the whole lattice when null).
+void write_xtr(Solver& s, const std::string& path, const std::string& fields, const std::string& offset_path,
+               const hb_selector* sel = nullptr);
 // Restore f_old = f_new from the "distributions" record with time `step`
 // (0 = the last record), then set the time step to that record's label.
 void read_checkpoint(Solver& s, const std::string& path, uint64_t step);

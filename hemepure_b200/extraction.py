@@ -1,0 +1,112 @@
+"""Property outputs of a case file: which fields of which sites go to which .xtr
+file at which steps.
+
+Restates SimConfig::DoIOForProperties / DoIOForPropertyOutputFile and the
+geometry readers (src/configuration/SimConfig.cc:409-564) and the write test
+LocalPropertyOutput::ShouldWrite (src/extraction/LocalPropertyOutput.cc:205-210).
+The records themselves are written by the library (`LBM.WriteXtr`).
+"""
+
+from __future__ import annotations
+
+import os
+import xml.etree.ElementTree as ET
+from dataclasses import dataclass
+from typing import List
+
+from . import lbm
+
+# Fields the library writes (OutputField types of the collide-and-stream path).
+WRITABLE_FIELDS = ("pressure", "velocity", "shearstress", "distributions")
+
+
+@dataclass
+class PropertyOutput:
+    file: str
+    period: int
+    start: int
+    stop: int
+    geometry: lbm.Selector
+    fields: List[str]
+
+    def due(self, time_step: int) -> bool:
+        """LocalPropertyOutput::ShouldWrite for a record labelled `time_step`."""
+        return self.start <= time_step <= self.stop and time_step % self.period == 0
+
+
+def _value(el, units: str) -> str:
+    if el is None:
+        raise ValueError("missing element")
+    if el.get("units") != units:
+        raise ValueError(f"invalid units for {el.tag}: expected {units!r}, got {el.get('units')!r}")
+    return el.get("value")
+
+
+def _vec(el, units: str):
+    s = _value(el, units).strip()
+    if not (s.startswith("(") and s.endswith(")")):
+        raise ValueError(f"bad vector {s!r}")
+    parts = [float(p) for p in s[1:-1].split(",")]
+    if len(parts) != 3:
+        raise ValueError(f"bad vector {s!r}")
+    return parts
+
+
+def _geometry(el) -> lbm.Selector:
+    kind = el.get("type")
+    if kind not in lbm.SELECTORS:
+        raise ValueError(f"Unrecognised property output geometry selector '{kind}'")
+    if kind == "plane":
+        radius_el = el.find("radius")
+        radius = float(_value(radius_el, "m")) if radius_el is not None else 0.0
+        return lbm.selector("plane", point=_vec(el.find("point"), "m"),
+                            normal=_vec(el.find("normal"), "dimensionless"), radius=radius)
+    if kind == "line":
+        points = el.findall("point")
+        if len(points) < 2:
+            raise ValueError("a line selector needs two <point> elements")
+        return lbm.selector("line", point=_vec(points[0], "m"), point2=_vec(points[1], "m"))
+    if kind in ("sphere", "surfaceWithinSphere"):
+        return lbm.selector(kind, point=_vec(el.find("point"), "m"), radius=float(_value(el.find("radius"), "m")))
+    if kind == "surfacepoint":
+        return lbm.selector(kind, point=_vec(el.find("point"), "m"))
+    return lbm.selector(kind)
+
+
+def property_outputs(xml_path: str) -> List[PropertyOutput]:
+    """The <propertyoutput> entries of a case file, in file order."""
+    root = ET.parse(xml_path).getroot()
+    props = root.find("properties")
+    out: List[PropertyOutput] = []
+    if props is None:
+        return out
+    for po in props.findall("propertyoutput"):
+        file = po.get("file")
+        if file is None or po.get("period") is None:
+            raise ValueError("a <propertyoutput> needs 'file' and 'period'")
+        geom = po.find("geometry")
+        if geom is None:
+            raise ValueError("a <propertyoutput> needs a <geometry>")
+        fields = []
+        for f in po.findall("field"):
+            kind = f.get("type")
+            if kind not in WRITABLE_FIELDS:
+                raise ValueError(f"field type '{kind}' is not written by this library")
+            fields.append(kind)
+        out.append(PropertyOutput(file=file, period=int(po.get("period")), start=int(po.get("start", 0)),
+                                  stop=int(po.get("stop", 1000000000)), geometry=_geometry(geom), fields=fields))
+    return out
+
+
+def write_due(sim: "lbm.LBM", outputs: List[PropertyOutput], directory: str) -> List[str]:
+    """Append a record to every output due for the step just completed; returns
+    the files written.  Outputs other than distributions need the step run with
+    the macroscopic caches filled."""
+    label = sim.time_step - 1
+    written = []
+    for o in outputs:
+        if o.due(label):
+            path = os.path.join(directory, o.file)
+            sim.WriteXtr(path, o.fields, geometry=o.geometry)
+            written.append(path)
+    return written

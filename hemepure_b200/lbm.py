@@ -42,7 +42,12 @@ EXPORTS = [
     "hb_batch_bytes", "hb_batch_create", "hb_batch_destroy", "hb_batch_add_xml", "hb_batch_add", "hb_batch_remove",
     "hb_batch_run", "hb_batch_get_macro", "hb_batch_member_info", "hb_batch_set_tuning", "hb_batch_stats",
     "hb_batch_prepare_xml", "hb_batch_prep_sites", "hb_batch_add_prepared", "hb_batch_prep_free",
+    "hb_write_xtr_selected", "hb_geometry_select",
 ]
+
+# Extraction geometry selectors (the <geometry type="..."> of a <propertyoutput>).
+SELECTORS = {"whole": 0, "plane": 1, "line": 2, "sphere": 3, "inlet": 4, "outlet": 5, "surface": 6,
+             "surfaceWithinSphere": 7, "surfacepoint": 8}
 
 
 class HemeLBError(RuntimeError):
@@ -72,6 +77,23 @@ class Params(C.Structure):
                 ("sponge_width", C.c_double), ("sponge_lifetime", C.c_uint64), ("initial_density", C.c_double),
                 ("initial_step", C.c_uint64), ("n_inlets", C.c_int), ("n_outlets", C.c_int),
                 ("inlets", Iolet * 16), ("outlets", Iolet * 16)]
+
+
+class Selector(C.Structure):
+    _fields_ = [("type", C.c_int), ("point", C.c_double * 3), ("point2", C.c_double * 3), ("normal", C.c_double * 3),
+                ("radius", C.c_double)]
+
+
+def selector(type: str = "whole", point=(0.0, 0.0, 0.0), point2=(0.0, 0.0, 0.0), normal=(0.0, 0.0, 1.0),
+             radius: float = 0.0) -> Selector:
+    """A geometry selector; points and radii in metres, as in the case file."""
+    s = Selector()
+    s.type = SELECTORS[type]
+    s.point[:] = [float(v) for v in point]
+    s.point2[:] = [float(v) for v in point2]
+    s.normal[:] = [float(v) for v in normal]
+    s.radius = float(radius)
+    return s
 
 
 class LatticeDesc(C.Structure):
@@ -112,6 +134,8 @@ def library() -> C.CDLL:
     L.hb_get_wk3.argtypes = [P, I, I, P]
     L.hb_get_tables.argtypes = [P, P, P, P, P, P, P, P]
     L.hb_write_xtr.argtypes = [P, C.c_char_p, C.c_char_p, C.c_char_p]
+    L.hb_write_xtr_selected.argtypes = [P, C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(Selector)]
+    L.hb_geometry_select.argtypes = [P, C.POINTER(Selector), C.c_double, P, P]
     L.hb_read_checkpoint.argtypes = [P, C.c_char_p, U64]
     L.hb_last_step_timing.argtypes = [P, P, P]
     L.hb_device_bytes.argtypes = [P, P]
@@ -301,9 +325,16 @@ class LBM:
             "neighbours", "wall_mask", "iolet_mask", "site_type", "iolet_id", "coords", "type_counts"))))
         return out
 
-    def WriteXtr(self, path: str, fields: Sequence[str], offset_path: Optional[str] = None) -> None:
-        self._check(library().hb_write_xtr(self._h, os.fspath(path).encode(), ",".join(fields).encode(),
-                                           os.fspath(offset_path).encode() if offset_path else None))
+    def WriteXtr(self, path: str, fields: Sequence[str], offset_path: Optional[str] = None,
+                 geometry: Optional[Selector] = None) -> None:
+        """Append one .xtr record (LocalPropertyOutput::Write) for the whole lattice,
+        or for the sites `geometry` (see `selector`) takes."""
+        off = os.fspath(offset_path).encode() if offset_path else None
+        if geometry is None:
+            self._check(library().hb_write_xtr(self._h, os.fspath(path).encode(), ",".join(fields).encode(), off))
+        else:
+            self._check(library().hb_write_xtr_selected(self._h, os.fspath(path).encode(), ",".join(fields).encode(),
+                                                        off, C.byref(geometry)))
 
     def ReadCheckpoint(self, path: str, step: int = 0) -> None:
         self._check(library().hb_read_checkpoint(self._h, os.fspath(path).encode(), int(step)))
@@ -372,6 +403,18 @@ class Geometry:
             raise HemeLBError(rc, last_create_error())
         out["dims"] = self.dims.copy()
         return out
+
+    def select(self, geometry: Selector, voxel_size: float, origin=(0.0, 0.0, 0.0)) -> np.ndarray:
+        """Mask (contiguous order) of the sites a geometry selector takes."""
+        n = C.c_int64()
+        dims = (C.c_int64 * 3)()
+        library().hb_geometry_site_count(self._g, C.byref(n), dims)
+        mask = np.zeros(n.value, np.uint8)
+        org = np.asarray(origin, dtype=np.float64)
+        rc = library().hb_geometry_select(self._g, C.byref(geometry), float(voxel_size), _p(org), _p(mask))
+        if rc != HB_OK:
+            raise HemeLBError(rc, last_create_error())
+        return mask.astype(bool)
 
     def layout(self, params: Params, wall: str = "SBB") -> Dict[str, int]:
         st = np.zeros(4, np.int64)

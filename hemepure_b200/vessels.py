@@ -519,7 +519,19 @@ def write_case_xml(path: str, gmy_name: str, vessel: Vessel, units: CaseUnits, s
         L.append('  <properties>')
         for po in properties:
             L.append(f'    <propertyoutput file="{po["file"]}" period="{int(po["period"])}">')
-            L.append(f'      <geometry type="{po.get("geometry", "whole")}" />')
+            geo = po.get("geometry", "whole")
+            if isinstance(geo, str):
+                L.append(f'      <geometry type="{geo}" />')
+            else:  # {"type": ..., "point": (m), "point2": (m), "normal": ..., "radius": m}
+                L.append(f'      <geometry type="{geo["type"]}">')
+                for key in ("point", "point2"):
+                    if key in geo:
+                        L.append(f'        <point units="m" value="{_vec(geo[key])}"/>')
+                if "normal" in geo:
+                    L.append(f'        <normal units="dimensionless" value="{_vec(geo["normal"])}"/>')
+                if "radius" in geo:
+                    L.append(f'        <radius units="m" value="{float(geo["radius"])!r}"/>')
+                L.append('      </geometry>')
             for fld in po["fields"]:
                 L.append(f'      <field type="{fld}" />')
             L.append('    </propertyoutput>')

@@ -182,6 +182,36 @@ int hb_get_tables(const hb_handle* h, int64_t* neighbours, uint32_t* wall_mask, 
  * "distributions"; comma-separated).  Appends a record if the file exists with
  * a matching header; `offset_path` (may be NULL) receives the .off file. */
 int hb_write_xtr(hb_handle* h, const char* path, const char* fields, const char* offset_path);
+/* Extraction geometry selectors (the <geometry type=...> of a <propertyoutput>,
+ * SimConfig::DoIOForPropertyOutputFile, src/configuration/SimConfig.cc:421-484):
+ * whole lattice; plane through `point` with `normal` (within half a voxel of it,
+ * and within `radius` of `point` when radius > 0); straight line from `point` to
+ * `point2`; sphere of `radius` about `point`; inlet or outlet sites; wall sites;
+ * wall sites in the sphere; wall sites within sqrt(3) voxels of `point`.  Points
+ * and radii in metres; the tests are made in the reference's float arithmetic
+ * (src/extraction/PlaneGeometrySelector.cc:54-81, StraightLineGeometrySelector.cc:30-49,
+ * SphereGeometrySelector.cc, SurfacePointSelector.cc:22-40). */
+enum {
+  HB_SELECT_WHOLE = 0,
+  HB_SELECT_PLANE = 1,
+  HB_SELECT_LINE = 2,
+  HB_SELECT_SPHERE = 3,
+  HB_SELECT_INLET = 4,
+  HB_SELECT_OUTLET = 5,
+  HB_SELECT_SURFACE = 6,
+  HB_SELECT_SURFACE_WITHIN_SPHERE = 7,
+  HB_SELECT_SURFACE_POINT = 8
+};
+typedef struct hb_selector {
+  int type;
+  double point[3];
+  double point2[3];
+  double normal[3];
+  double radius;
+} hb_selector;
+/* hb_write_xtr restricted to the sites `sel` takes (header site count included). */
+int hb_write_xtr_selected(hb_handle* h, const char* path, const char* fields, const char* offset_path,
+                          const hb_selector* sel);
 /* Restore f from the "distributions" field of an .xtr at time step `step`
  * (LocalDistributionInput::LoadDistribution). */
 int hb_read_checkpoint(hb_handle* h, const char* path, uint64_t step);
@@ -250,6 +280,10 @@ int hb_geometry_tables(const hb_geometry* g, int64_t* neighbours, uint32_t* wall
 /* Device layout summary without allocating: run axis, runs, plain bulk sites,
  * general sites (or an error if the lattice cannot be streamed exactly). */
 int hb_geometry_layout(const hb_geometry* g, const hb_params* params, int wall, int64_t stats[4]);
+/* The selector's site mask over the geometry (contiguous order; 1 = taken), for a
+ * voxel size and origin in metres.  Host-only. */
+int hb_geometry_select(const hb_geometry* g, const hb_selector* sel, double voxel_size, const double origin[3],
+                       uint8_t* mask);
 int hb_geometry_close(hb_geometry* g);
 
 /* ---- without device allocation --------------------------------------------------- */

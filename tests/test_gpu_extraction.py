@@ -156,3 +156,30 @@ def test_checkpoint_rejects_a_missing_step_and_a_wrong_lattice(case_dir, tmp_pat
     with pytest.raises(lbm.HemeLBError) as e:
         c.ReadCheckpoint(path)
     assert e.value.code == -3
+
+
+def test_selected_record_is_the_whole_record_restricted(case_dir, tmp_path):
+    """A record for a plane or a sphere holds exactly the sites the selector takes,
+    with the same values as the whole-lattice record at those sites."""
+    xml, gmy, info, kernel, wall, _ = make_small_case(case_dir, "pipe_bfl")
+    sim = lbm.LBM(xml, kernel=kernel, wall=wall)
+    sim.step(30, macro=True)
+    fields = ["pressure", "velocity", "shearstress"]
+    sim.WriteXtr(tmp_path / "whole.xtr", fields)
+    (_, wcoords, wvals), = read_xtr(tmp_path / "whole.xtr")["records"]
+    dx = units(xml, kernel)[0]
+    lo, hi = wcoords.min(0), wcoords.max(0)
+    mid = (lo + hi) / 2.0 * dx
+    geo = lbm.Geometry(gmy)
+    for sel in (lbm.selector("plane", point=mid, normal=(0, 0, 1)),
+                lbm.selector("sphere", point=mid, radius=0.6 * (hi[0] - lo[0]) / 2.0 * dx),
+                lbm.selector("surface")):
+        path = tmp_path / f"sel{sel.type}.xtr"
+        sim.WriteXtr(path, fields, geometry=sel)
+        x = read_xtr(path)
+        mask = geo.select(sel, dx, (0.0, 0.0, 0.0))
+        assert x["nsites"] == int(mask.sum()) > 0
+        (label, coords, vals), = x["records"]
+        assert np.array_equal(coords, wcoords[mask])
+        for f in fields:
+            assert np.array_equal(vals[f], wvals[f][mask])
