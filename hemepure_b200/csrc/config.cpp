@@ -2,7 +2,8 @@
 //
 // Case file: src/configuration/SimConfig.cc:84-198 (simulation), 262-408 (iolets),
 // 640-655 (iolet position/normal), 668-723 (initial conditions, sponge),
-// 725-754 (cosine), 796-824 (WK3), 856-876 (parabolic); unit conversion
+// 725-754 (cosine), 756-794 (file, WK2), 796-824 (WK3), 856-876 (parabolic); the
+// file iolet's density table src/lb/iolets/InOutLetFile.cc:48-127; unit conversion
 // src/util/UnitConverter.cc:15-118 and UnitConverter.h:153-203; tau from
 // src/lb/LbmParameters.h:29-37.
 //
@@ -14,10 +15,12 @@
 
 #include <zlib.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <map>
 
 #include "xml.h"
 
@@ -84,6 +87,58 @@ struct Units {
   }
 };
 
+// util::NumericalFunctions::LinearInterpolate (src/util/utilityFunctions.h:96-134).
+double linear_interpolate(const std::vector<double>& xs, const std::vector<double>& ys, double x) {
+  size_t i = 0;
+  while (!(x >= xs[i] && x <= xs[i + 1])) {
+    i++;
+    if (i + 1 >= xs.size()) throw Error{HB_ERR_FORMAT, "file iolet: interpolation beyond the file's time range"};
+  }
+  return ys[i] + (x - xs[i]) / (xs[i + 1] - xs[i]) * (ys[i + 1] - ys[i]);
+}
+
+// InOutLetFile::CalculateTable: the lattice density at every step 0..total_steps
+// from a file of (time in s, pressure in mmHg) pairs, and the minimum density.
+void file_density_table(const std::string& path, uint64_t total_steps, double dt, const Units& u,
+                        std::vector<double>& table, double& density_min) {
+  std::ifstream in(path);
+  if (!in) throw Error{HB_ERR_IO, "cannot open iolet file " + path};
+  std::map<double, double> pairs;
+  double t = 0.0, v = 0.0;
+  while (in.good()) {  // the reference's read loop, with its end-of-file behaviour
+    in >> t >> v;
+    pairs[t] = v;
+  }
+  std::vector<double> times, values;
+  double pmin = pairs.begin()->second, pmax = pmin;
+  const double end = (double)total_steps * dt;
+  for (const auto& e : pairs) {
+    if (e.first > end) {
+      if (times.empty()) throw Error{HB_ERR_FORMAT, "file iolet: the file starts after the simulation ends"};
+      const double ratio = (end - times.back()) / (e.first - times.back());
+      const double final_p = values.back() + ratio * (e.second - values.back());
+      times.push_back(end);
+      pmin = std::min(pmin, final_p);
+      pmax = std::max(pmax, final_p);
+      values.push_back(final_p);
+      break;
+    }
+    pmin = std::min(pmin, e.second);
+    pmax = std::max(pmax, e.second);
+    times.push_back(e.first);
+    values.push_back(e.second);
+  }
+  density_min = u.pressure_abs(pmin) / kCs2;
+  const int period = (int)(times.back() / dt);
+  if (period <= 0 || total_steps == 0) throw Error{HB_ERR_FORMAT, "file iolet: the file spans less than one step"};
+  table.resize(total_steps + 1);
+  for (uint64_t ts = 0; ts <= total_steps; ts++) {
+    const double point =
+        times.front() + ((double)(ts % (uint64_t)period) / (double)total_steps) * (times.back() - times.front());
+    table[ts] = u.pressure_abs(linear_interpolate(times, values, point)) / kCs2;
+  }
+}
+
 void normalise(double n[3]) {
   if (n[0] == 0.0 && n[1] == 0.0 && n[2] == 0.0) return;
   const double m = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
@@ -147,7 +202,7 @@ CaseConfig read_case(const std::string& xml_path, int kernel) {
     p.sponge_lifetime = parse_u64(dim_value(sp.require("lifetime"), "lattice"), "lifetime");
   }
 
-  auto read_iolets = [&](const char* group, hb_iolet* out, int& count) {
+  auto read_iolets = [&](const char* group, hb_iolet* out, int& count, int group_index) {
     const XmlElement& g = root->require(group);
     std::string child = std::string(group).substr(0, std::strlen(group) - 1);
     count = 0;
@@ -177,6 +232,23 @@ CaseConfig read_case(const std::string& xml_path, int kernel) {
         io.cp = parse_double(dim_value(cond.require("Cp"), "m^4*s^2/kg"), "Cp") * cf;
         io.radius = u.to_lattice("m", parse_double(dim_value(cond.require("radius"), "m"), "radius"));
         io.area = parse_double(dim_value(cond.require("area"), "m^2"), "area") / (c.dx * c.dx);
+      } else if (type == "pressure" && sub == "WK2") {
+        io.kind = kWK2;
+        io.rp = parse_double(dim_value(cond.require("R"), "kg/m^4*s"), "R") * ((c.dt * c.dx) / kBloodDensity);
+        io.cp = parse_double(dim_value(cond.require("C"), "m^4*s^2/kg"), "C") * (kBloodDensity / (c.dt * c.dt * c.dx));
+        io.radius = u.to_lattice("m", parse_double(dim_value(cond.require("radius"), "m"), "radius"));
+        io.area = parse_double(dim_value(cond.require("area"), "m^2"), "area") / (c.dx * c.dx);
+      } else if (type == "pressure" && sub == "file") {
+        io.kind = kFile;
+        std::string path = cond.require("path").attr("value");
+        if (!path.empty() && path[0] != '/') {
+          const size_t slash = xml_path.rfind('/');
+          if (slash != std::string::npos) path = xml_path.substr(0, slash + 1) + path;
+        }
+        std::vector<double>& table = c.tables[group_index * 16 + (count - 1)];
+        file_density_table(path, c.total_steps, c.dt, u, table, io.density_min);
+        io.density_table = table.data();
+        io.table_steps = table.size();
       } else if (type == "velocity" && sub == "parabolic") {
         io.kind = kParabolic;
         io.radius = u.to_lattice("m", parse_double(dim_value(cond.require("radius"), "m"), "radius"));
@@ -187,8 +259,8 @@ CaseConfig read_case(const std::string& xml_path, int kernel) {
       }
     }
   };
-  read_iolets("inlets", p.inlets, p.n_inlets);
-  read_iolets("outlets", p.outlets, p.n_outlets);
+  read_iolets("inlets", p.inlets, p.n_inlets, 0);
+  read_iolets("outlets", p.outlets, p.n_outlets, 1);
 
   if (const XmlElement* props = root->child("properties")) {
     for (const XmlElement* po : props->all("propertyoutput")) {

@@ -27,6 +27,7 @@ struct CaseConfig {
     std::vector<std::string> fields;
   };
   std::vector<PropertyOutput> outputs;
+  std::vector<double> tables[32];  // file iolets' density tables (inlets 0-15, outlets 16-31)
   std::string checkpoint_file;    // <initialconditions><checkpoint file=...>
   bool has_time = false;          // <initialconditions><time> present
 };

@@ -30,14 +30,15 @@ struct IoletDev {
   uint64_t warmup;
 };
 
-struct WK3Dev {           // InOutLetWK3 state
+struct WK3Dev {           // InOutLetWK3 / InOutLetWK2 state
   double density, density_new, flow, flow_old;
-  double rc, rp, cp, area;
+  double rc, rp, cp, area;    // WK2: rp is R, cp is C
   int cpl_start, cpl_count;   // coupling slots of this iolet
   int count_prev;             // coupling sites summed at the previous step (0 before the first)
   int centre_couples;         // the centre site takes part in the coupling
   int iolet;                  // index into the iolet table
-  int pad[3];
+  int kind;                   // kWK3 or kWK2
+  int pad[2];
 };
 
 struct GeneralDev {

@@ -41,7 +41,7 @@ constexpr double kNoValue = 1.7976931348623157e308;  // std::numeric_limits<doub
 
 enum Kernel { kLBGK = 0, kTRT = 1, kLES = 2 };
 enum Wall { kSBB = 0, kBFL = 1, kGZS = 2 };
-enum IoletKind { kCosine = 0, kWK3 = 1, kParabolic = 2 };
+enum IoletKind { kCosine = 0, kWK3 = 1, kParabolic = 2, kWK2 = 3, kFile = 4 };
 
 // Host-side error carrying one of the HB_ERR_* codes.
 struct Error {

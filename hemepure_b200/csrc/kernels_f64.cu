@@ -104,11 +104,19 @@ __global__ void k_wk3_begin(WK3Dev* wk3, const double* cpl_buf, double* dens_row
     double d_after = density, flow_old = W.flow_old;
     if (W.centre_couples) {
       const double pressure = density * kCs2;
-      const double Rc = W.rc, Rp = W.rp, Cp = W.cp;
-      const double pn = (Rp * Cp * pressure + (Rc + Rp) * (2.0 * flow - W.flow_old) + Rc * Rp * Cp * (flow - W.flow_old)) / (1.0 + Rp * Cp);
-      W.density_new = pn / kCs2;
-      d_after = W.density_new;
-      flow_old = flow;
+      if (W.kind == kWK2) {
+        // InOutLetWK2::DoPreStreamCoupling / DoPostStreamCoupling (InOutLetWK2.cc:66-95).
+        const double R0 = W.rp, C0 = W.cp;
+        const double pn = R0 / (1.0 + R0 * C0) * (flow + C0 * pressure);
+        W.density_new = pn / kCs2;
+        d_after = W.density_new;
+      } else {
+        const double Rc = W.rc, Rp = W.rp, Cp = W.cp;
+        const double pn = (Rp * Cp * pressure + (Rc + Rp) * (2.0 * flow - W.flow_old) + Rc * Rp * Cp * (flow - W.flow_old)) / (1.0 + Rp * Cp);
+        W.density_new = pn / kCs2;
+        d_after = W.density_new;
+        flow_old = flow;
+      }
     }
     W.density = d_after;
     W.flow = flow;

@@ -218,7 +218,7 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
       const int idx = grp * 16 + id;
       L.g_io[g] = idx;
       const int kind = iolet_cfg(idx).kind;
-      if (kind == kWK3) {
+      if (kind == kWK3 || kind == kWK2) {
         bool couples = false;
         for (int d = 1; d < Q; d++)
           if (((L.g_iolet[g] >> (d - 1)) & 1u) && inv(d) == L.dir0[idx]) couples = true;
@@ -243,7 +243,7 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
   int slot = 0;
   for (int idx = 0; idx < 32; idx++) {
     const int cnt = idx < 16 ? p.n_inlets : p.n_outlets;
-    if ((idx % 16) >= cnt || iolet_cfg(idx).kind != kWK3) continue;
+    if ((idx % 16) >= cnt || (iolet_cfg(idx).kind != kWK3 && iolet_cfg(idx).kind != kWK2)) continue;
     auto& v = cpl_sites[idx];
     std::sort(v.begin(), v.end());
     Layout::Coupling c;

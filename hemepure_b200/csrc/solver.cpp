@@ -75,7 +75,18 @@ Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& 
   if (!(p_.tau > 0.5)) throw Error{HB_ERR_ARG, "tau must exceed 1/2"};
   for (int k = 0; k < p_.n_inlets + p_.n_outlets; k++) {
     const hb_iolet& io = k < p_.n_inlets ? p_.inlets[k] : p_.outlets[k - p_.n_inlets];
-    if (io.kind < 0 || io.kind > 2) throw Error{HB_ERR_ARG, "unknown iolet kind"};
+    if (io.kind < 0 || io.kind > kFile) throw Error{HB_ERR_ARG, "unknown iolet kind"};
+    if (io.kind == kFile && (!io.density_table || io.table_steps == 0))
+      throw Error{HB_ERR_ARG, "a file iolet needs its density table"};
+  }
+  // The file iolets' density tables are the caller's only for the call: keep copies.
+  for (int idx = 0; idx < 32; idx++) {
+    const int cnt = idx < 16 ? p_.n_inlets : p_.n_outlets;
+    if (idx % 16 >= cnt) continue;
+    hb_iolet& io = idx < 16 ? p_.inlets[idx] : p_.outlets[idx - 16];
+    if (io.kind != kFile) continue;
+    tables_[idx].assign(io.density_table, io.density_table + io.table_steps);
+    io.density_table = tables_[idx].data();
   }
   if ((opt_.wall == kBFL || opt_.wall == kGZS) && t_.q.empty()) throw Error{HB_ERR_ARG, "BFL and GZS walls need wall distances"};
   check(cudaSetDevice(opt_.device), "cudaSetDevice");
@@ -184,6 +195,7 @@ void Solver::upload() {
     std::memset(&w, 0, sizeof(w));
     w.density = w.density_new = 1.0;
     w.flow = w.flow_old = 0.0;
+    w.kind = cfg.kind;
     w.rc = cfg.rc;
     w.rp = cfg.rp;
     w.cp = cfg.cp;
@@ -279,7 +291,8 @@ void Solver::fill_density_rows(uint64_t t_first, int count) {
   double mind = 1.7976931348623157e308;
   for (int k = 0; k < p_.n_inlets + p_.n_outlets; k++) {
     const hb_iolet& c = k < p_.n_inlets ? p_.inlets[k] : p_.outlets[k - p_.n_inlets];
-    const double dmin = c.kind == kCosine ? c.density_mean - c.density_amp : 1.0;
+    // InOutLet::GetDensityMin: cosine mean - amplitude, file its table's minimum, others 1.
+    const double dmin = c.kind == kCosine ? c.density_mean - c.density_amp : c.kind == kFile ? c.density_min : 1.0;
     if (dmin < mind) mind = dmin;
   }
   for (int r = 0; r < count; r++) {
@@ -298,6 +311,10 @@ void Solver::fill_density_rows(uint64_t t_first, int count) {
             v = fac * target + (1. - fac) * mind;
           }
         }
+      }
+      if (idx % 16 < cnt) {
+        const hb_iolet& c = idx < 16 ? p_.inlets[idx] : p_.outlets[idx - 16];
+        if (c.kind == kFile) v = c.density_table[t0 < c.table_steps ? t0 : c.table_steps - 1];
       }
       host_rows_[(size_t)r * 32 + idx] = v;
     }

@@ -82,6 +82,7 @@ class Solver {
 
   LatticeTables t_;
   hb_params p_;
+  std::vector<double> tables_[32];  // file iolets' density tables (p_ points into them)
   hb_options opt_;
   Layout L_;
   cudaStream_t stream_ = nullptr;

@@ -444,6 +444,19 @@ class WK3BC:
     radius: Optional[float] = None
 
 
+@dataclass
+class WK2BC:
+    r: float        # lattice units
+    c: float
+    area: float     # lattice units
+    radius: Optional[float] = None
+
+
+@dataclass
+class FilePressureBC:
+    path: str       # (time in s, pressure in mmHg) pairs, one per line; relative to the case file
+
+
 def write_case_xml(path: str, gmy_name: str, vessel: Vessel, units: CaseUnits, steps: int,
                    inlet_bcs: Sequence, outlet_bcs: Sequence, warmup: int = 0,
                    relaxation_parameter: Optional[float] = None, sponge: Optional[dict] = None,
@@ -508,6 +521,20 @@ def write_case_xml(path: str, gmy_name: str, vessel: Vessel, units: CaseUnits, s
                 L.append(f'        <Cp units="m^4*s^2/kg" value="{bc.c_p / cap!r}"/>')
                 L.append(f'        <radius units="m" value="{float(r) * units.voxel!r}"/>')
                 L.append(f'        <area units="m^2" value="{bc.area * units.voxel * units.voxel!r}"/>')
+                L.append('      </condition>')
+            elif isinstance(bc, WK2BC):
+                r = io.radius if bc.radius is None else bc.radius
+                res = (units.dt * units.voxel) / BLOOD_DENSITY
+                cap = BLOOD_DENSITY / (units.dt * units.dt * units.voxel)
+                L.append('      <condition subtype="WK2" type="pressure">')
+                L.append(f'        <R units="kg/m^4*s" value="{bc.r / res!r}"/>')
+                L.append(f'        <C units="m^4*s^2/kg" value="{bc.c / cap!r}"/>')
+                L.append(f'        <radius units="m" value="{float(r) * units.voxel!r}"/>')
+                L.append(f'        <area units="m^2" value="{bc.area * units.voxel * units.voxel!r}"/>')
+                L.append('      </condition>')
+            elif isinstance(bc, FilePressureBC):
+                L.append('      <condition subtype="file" type="pressure">')
+                L.append(f'        <path value="{bc.path}"/>')
                 L.append('      </condition>')
             else:
                 raise TypeError(bc)

@@ -52,6 +52,8 @@ extern "C" {
 #define HB_IOLET_COSINE 0        /* Nash pressure, src/lb/iolets/InOutLetCosine.cc */
 #define HB_IOLET_WK3 1           /* Nash pressure, src/lb/iolets/InOutLetWK3.cc */
 #define HB_IOLET_PARABOLIC 2     /* Ladd velocity, src/lb/iolets/InOutLetParabolicVelocity.cc */
+#define HB_IOLET_WK2 3           /* Nash pressure, src/lb/iolets/InOutLetWK2.cc (R in rp, C in cp) */
+#define HB_IOLET_FILE 4          /* Nash pressure from a time-pressure file, src/lb/iolets/InOutLetFile.cc */
 
 /* ---- storage precision of the distributions */
 #define HB_STORE_FP64 0          /* plain form: FP64 storage and arithmetic */
@@ -78,7 +80,14 @@ typedef struct hb_iolet {
   double density_mean, density_amp, phase, period; /* cosine (InOutLetCosine) */
   uint64_t warmup;          /* extra_warmup_steps */
   double radius, max_speed; /* parabolic (InOutLetParabolicVelocity) */
-  double rc, rp, cp, area;  /* WK3 (InOutLetWK3) */
+  double rc, rp, cp, area;  /* WK3 (InOutLetWK3); WK2 (InOutLetWK2) uses rp as R and cp as C */
+  /* file pressure (InOutLetFile): lattice density per 0-indexed step (its densityTable;
+   * steps beyond the table take its last entry) and the table's minimum density.  The
+   * library copies the table when a handle is created; hb_read_case leaves it NULL
+   * (hb_read_case_iolet_table fills a caller buffer). */
+  const double* density_table;
+  uint64_t table_steps;
+  double density_min;
 } hb_iolet;
 
 /* LbmParameters + iolet set + initial condition, all in lattice units. */
@@ -268,6 +277,9 @@ int hb_batch_stats(const hb_batch* b, double* last_block_ms, int64_t* active_sit
 /* SimConfig::DoIO for the collide-and-stream path: lattice-unit parameters and
  * the geometry path (resolved against the case file's directory). */
 int hb_read_case(const char* xml_path, int kernel, hb_params* params, char* gmy_path, size_t gmy_path_len);
+/* The density table of a file-pressure iolet of a case (`outlet` 0 for inlets,
+ * 1 for outlets; `index` within the group): its first `count` entries. */
+int hb_read_case_iolet_table(const char* xml_path, int kernel, int outlet, int index, double* out, uint64_t count);
 
 typedef struct hb_geometry hb_geometry;
 /* GeometryReader + LatticeData on one rank: the reference-order tables. */

@@ -7,7 +7,8 @@ other:
 * `src/configuration/SimConfig.cc:84-198` (simulation section, extra warm-up steps),
   `:262-408` (iolets), `:640-655` (iolet position in lattice units, normalised normal),
   `:668-723` (initial conditions, sponge layer), `:725-754` (cosine),
-  `:796-824` (WK3), `:856-876` (parabolic);
+  `:756-794` (file pressure, WK2), `:796-824` (WK3), `:856-876` (parabolic);
+* `src/lb/iolets/InOutLetFile.cc:48-127` (the file iolet's density table);
 * `src/util/UnitConverter.cc:15-118`, `src/util/UnitConverter.h:153-203`;
 * `src/lb/LbmParameters.h:29-37` (tau from dt and dx), `src/constants.h`.
 """
@@ -98,6 +99,8 @@ class IoletCfg:
     rp: float = 0.0
     cp: float = 0.0
     area: float = 0.0
+    table: Optional[List[float]] = None   # file pressure: density per 0-indexed step
+    density_min: float = 0.0
 
 
 @dataclass
@@ -116,6 +119,58 @@ class CaseCfg:
     outlets: List[IoletCfg] = field(default_factory=list)
     dt: float = 0.0
     dx: float = 0.0
+
+
+def _read_time_value_pairs(path: str):
+    """`while (file.good()) { file >> t >> v; pairs[t] = v; }`: a file whose last
+    number is followed by whitespace makes one more pass, in which the stream
+    reaches its end while skipping whitespace, so neither extraction runs and
+    the last pair is stored again unchanged."""
+    tokens = open(path).read().split()
+    pairs = {}
+    for k in range(0, len(tokens) - 1, 2):
+        pairs[float(tokens[k])] = float(tokens[k + 1])
+    return pairs
+
+
+def _linear_interpolate(xs, ys, x):
+    """util::NumericalFunctions::LinearInterpolate (src/util/utilityFunctions.h:96-134)."""
+    i = 0
+    while not (x >= xs[i] and x <= xs[i + 1]):
+        i += 1
+        if i + 1 >= len(xs):
+            raise ValueError("interpolation beyond the file's time range")
+    return ys[i] + (x - xs[i]) / (xs[i + 1] - xs[i]) * (ys[i + 1] - ys[i])
+
+
+def file_density_table(path: str, total_steps: int, dt: float, u: "Units"):
+    """InOutLetFile::CalculateTable (src/lb/iolets/InOutLetFile.cc:48-127): the
+    lattice density at every step 0..total_steps, and the minimum density."""
+    pairs = _read_time_value_pairs(path)
+    times, values = [], []
+    entries = sorted(pairs.items())
+    p_min = p_max = entries[0][1]
+    end = total_steps * dt
+    for t, v in entries:
+        if t > end:
+            ratio = (end - times[-1]) / (t - times[-1])
+            final = values[-1] + ratio * (v - values[-1])
+            times.append(end)
+            p_min, p_max = min(p_min, final), max(p_max, final)
+            values.append(final)
+            break
+        p_min, p_max = min(p_min, v), max(p_max, v)
+        times.append(t)
+        values.append(v)
+    density_min = u.pressure_to_lattice(p_min) / CS2
+    period_steps = int(times[-1] / dt)
+    if period_steps <= 0:
+        raise ValueError("the file's time range is shorter than one step")
+    table = []
+    for step in range(total_steps + 1):
+        point = times[0] + (float(step % period_steps) / float(total_steps)) * (times[-1] - times[0])
+        table.append(u.pressure_to_lattice(_linear_interpolate(times, values, point)) / CS2)
+    return table, density_min
 
 
 def _normalised(v):
@@ -186,6 +241,17 @@ def load_case(xml_path: str, kernel: str = "LBGK") -> CaseCfg:
                 io.cp = u.capacitance(_val(cond.find("Cp"), "m^4*s^2/kg"))
                 io.radius = u.to_lattice("m", _val(cond.find("radius"), "m"))
                 io.area = u.area(_val(cond.find("area"), "m^2"))
+            elif typ == "pressure" and sub == "WK2":
+                io = IoletCfg("wk2", pos, nrm)
+                io.rp = u.resistance(_val(cond.find("R"), "kg/m^4*s"))
+                io.cp = u.capacitance(_val(cond.find("C"), "m^4*s^2/kg"))
+                io.radius = u.to_lattice("m", _val(cond.find("radius"), "m"))
+                io.area = u.area(_val(cond.find("area"), "m^2"))
+            elif typ == "pressure" and sub == "file":
+                io = IoletCfg("file", pos, nrm)
+                path = cond.find("path").get("value")
+                path = os.path.normpath(os.path.join(os.path.dirname(os.path.abspath(xml_path)), path))
+                io.table, io.density_min = file_density_table(path, steps, dt, u)
             elif typ == "velocity" and sub == "parabolic":
                 io = IoletCfg("parabolic", pos, nrm)
                 io.radius = u.to_lattice("m", _val(cond.find("radius"), "m"))

@@ -538,9 +538,13 @@ static double cosine_density(const iolet_t* io, uint64_t t0) {
 
 static double iolet_density(const iolet_t* io, uint64_t t0) {
   if (io->cfg.kind == ORC_IOLET_COSINE) return cosine_density(io, t0);
-  if (io->cfg.kind == ORC_IOLET_WK3) return io->density;
+  if (io->cfg.kind == ORC_IOLET_WK3 || io->cfg.kind == ORC_IOLET_WK2) return io->density;
+  if (io->cfg.kind == ORC_IOLET_FILE) /* InOutLetFile::GetDensity: densityTable[timeStep] */
+    return io->cfg.table[t0 < io->cfg.table_len ? t0 : io->cfg.table_len - 1];
   return 1.0; /* InOutLetVelocity::GetDensity */
 }
+
+static int is_windkessel(const iolet_t* io) { return io->cfg.kind == ORC_IOLET_WK3 || io->cfg.kind == ORC_IOLET_WK2; }
 
 /* InOutLetParabolicVelocity::GetVelocity.  Returns 0, or -1 for a point
  * outside the iolet radius (the reference exits with code 16). */
@@ -640,7 +644,9 @@ int orc_sim_create(const orc_lattice* lat, const orc_params* p, orc_sim** out, c
     for (int k = 0; k < s->nio[g]; k++) {
       iolet_t* io = &s->io[g][k];
       io->cfg = g == 0 ? p->inlets[k] : p->outlets[k];
-      double dmin = io->cfg.kind == ORC_IOLET_COSINE ? io->cfg.density_mean - io->cfg.density_amp : 1.0;
+      /* GetDensityMin: cosine mean - amplitude, file its table's minimum, others 1 */
+      double dmin = io->cfg.kind == ORC_IOLET_COSINE ? io->cfg.density_mean - io->cfg.density_amp
+                    : io->cfg.kind == ORC_IOLET_FILE ? io->cfg.density_min : 1.0;
       if (dmin < mind) mind = dmin;
       for (int d = 0; d < 3; d++) io->normal_f[d] = (float)io->cfg.normal[d];
       sort_dirs_close_to_normal(io);
@@ -951,11 +957,11 @@ int orc_sim_run(orc_sim* s, int64_t steps, int want_macro) {
 #endif
   for (int64_t st = 0; st < steps; st++) {
     const int macro = want_macro && st == steps - 1;
-    /* BeginPhase: WK3 DoComms (self-message and flow-rate reduction on one rank). */
+    /* BeginPhase: WK3/WK2 DoComms (self-message and flow-rate reduction on one rank). */
     for (int g = 0; g < 2; g++)
       for (int k = 0; k < s->nio[g]; k++) {
         iolet_t* io = &s->io[g][k];
-        if (io->cfg.kind != ORC_IOLET_WK3) continue;
+        if (!is_windkessel(io)) continue;
         io->density = io->density_new;
         io->flow = io->flow_new;
         if (io->count != 0) io->flow = io->flow * io->cfg.area / (double)io->count;
@@ -970,12 +976,19 @@ int orc_sim_run(orc_sim* s, int64_t steps, int want_macro) {
       if (!s->cpl_flag[i]) continue;
       const int grp = l->stype[i] == 1 ? 0 : 1;
       iolet_t* io = &s->io[grp][l->iolet_id[i]];
-      if (io->cfg.kind != ORC_IOLET_WK3) continue;
+      if (!is_windkessel(io)) continue;
       if (i == io->centre) {
         const double pressure = io->density * CS2;
-        const double Rc = io->cfg.rc, Rp = io->cfg.rp, Cp = io->cfg.cp;
-        const double pn = (Rp * Cp * pressure + (Rc + Rp) * (2.0 * io->flow - io->flow_old) + Rc * Rp * Cp * (io->flow - io->flow_old)) / (1.0 + Rp * Cp);
-        io->density_new = pn / CS2;
+        if (io->cfg.kind == ORC_IOLET_WK3) {
+          const double Rc = io->cfg.rc, Rp = io->cfg.rp, Cp = io->cfg.cp;
+          const double pn = (Rp * Cp * pressure + (Rc + Rp) * (2.0 * io->flow - io->flow_old) + Rc * Rp * Cp * (io->flow - io->flow_old)) / (1.0 + Rp * Cp);
+          io->density_new = pn / CS2;
+        } else {
+          /* InOutLetWK2::DoPreStreamCoupling (InOutLetWK2.cc:66-82) */
+          const double R0 = io->cfg.rp, C0 = io->cfg.cp;
+          const double pn = R0 / (1.0 + R0 * C0) * (io->flow + C0 * pressure);
+          io->density_new = pn / CS2;
+        }
       }
       const double* nrm = io->cfg.normal;
       io->flow_new += s->cpl_u[3 * i] * (-nrm[0]) + s->cpl_u[3 * i + 1] * (-nrm[1]) + s->cpl_u[3 * i + 2] * (-nrm[2]);
@@ -987,10 +1000,10 @@ int orc_sim_run(orc_sim* s, int64_t steps, int want_macro) {
     for (int g = 0; g < 2; g++)
       for (int k = 0; k < s->nio[g]; k++) {
         iolet_t* io = &s->io[g][k];
-        if (io->cfg.kind != ORC_IOLET_WK3 || io->centre < 0) continue;
+        if (!is_windkessel(io) || io->centre < 0) continue;
         if (s->cpl_flag[io->centre] && l->iolet_id[io->centre] == k && (l->stype[io->centre] == 1 ? 0 : 1) == g) {
           io->density = io->density_new;
-          io->flow_old = io->flow;
+          if (io->cfg.kind == ORC_IOLET_WK3) io->flow_old = io->flow;
         }
       }
     /* EndIteration: swap. */

@@ -23,7 +23,7 @@ enum { ORC_LBGK = 0, ORC_TRT = 1, ORC_LBGKLES = 2 };
 /* Wall streamers (SimpleBounceBackDelegate.h, BouzidiFirdaousLallemandDelegate.h, GuoZhengShiDelegate.h). */
 enum { ORC_SBB = 0, ORC_BFL = 1, ORC_GZS = 2 };
 /* Iolet streamers and iolet value sources. */
-enum { ORC_IOLET_COSINE = 0, ORC_IOLET_WK3 = 1, ORC_IOLET_PARABOLIC = 2 };
+enum { ORC_IOLET_COSINE = 0, ORC_IOLET_WK3 = 1, ORC_IOLET_PARABOLIC = 2, ORC_IOLET_WK2 = 3, ORC_IOLET_FILE = 4 };
 
 typedef struct orc_iolet {
   int kind;                 /* ORC_IOLET_* */
@@ -34,8 +34,12 @@ typedef struct orc_iolet {
   uint64_t warmup;
   /* parabolic */
   double radius, max_speed;
-  /* WK3 (lattice units) */
+  /* WK3 (lattice units); WK2 uses rp as its R and cp as its C */
   double rc, rp, cp, area;
+  /* file pressure: density per 0-indexed step (InOutLetFile densityTable) and its minimum */
+  const double* table;
+  uint64_t table_len;
+  double density_min;
 } orc_iolet;
 
 typedef struct orc_params {

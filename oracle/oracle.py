@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "_build", "libhboracle.so")
 
 KERNELS = {"LBGK": 0, "TRT": 1, "LBGKLESSL": 2}
 WALLS = {"SBB": 0, "BFL": 1, "GZS": 2}
-IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2}
+IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2, "wk2": 3, "file": 4}
 
 
 def build(force: bool = False) -> str:
@@ -43,7 +43,7 @@ class _Iolet(C.Structure):
                 ("density_mean", C.c_double), ("density_amp", C.c_double), ("phase", C.c_double),
                 ("period", C.c_double), ("warmup", C.c_uint64), ("radius", C.c_double),
                 ("max_speed", C.c_double), ("rc", C.c_double), ("rp", C.c_double), ("cp", C.c_double),
-                ("area", C.c_double)]
+                ("area", C.c_double), ("table", C.c_void_p), ("table_len", C.c_uint64), ("density_min", C.c_double)]
 
 
 class _Params(C.Structure):
@@ -144,7 +144,9 @@ class Lattice:
         return a
 
 
-def make_params(cfg: case_mod.CaseCfg, kernel: str, wall: str) -> _Params:
+def make_params(cfg: case_mod.CaseCfg, kernel: str, wall: str, keep: Optional[list] = None) -> _Params:
+    """The oracle's parameter block; file iolets' density tables are appended to
+    `keep`, which must outlive the simulation that uses them."""
     p = _Params()
     p.kernel = KERNELS[kernel]
     p.wall = WALLS[wall]
@@ -165,6 +167,13 @@ def make_params(cfg: case_mod.CaseCfg, kernel: str, wall: str) -> _Params:
             d.warmup = io.warmup
             d.radius, d.max_speed = io.radius, io.max_speed
             d.rc, d.rp, d.cp, d.area = io.rc, io.rp, io.cp, io.area
+            if io.table is not None:
+                tab = np.ascontiguousarray(io.table, dtype=np.float64)
+                if keep is not None:
+                    keep.append(tab)
+                d.table = tab.ctypes.data
+                d.table_len = len(tab)
+                d.density_min = io.density_min
     p.n_inlets = len(cfg.inlets)
     p.n_outlets = len(cfg.outlets)
     return p
@@ -178,7 +187,8 @@ class Simulation:
         self.cfg = case_mod.load_case(xml_path, kernel)
         self.lattice = lattice or Lattice(self.cfg.gmy_path)
         self.n = self.lattice.n
-        params = make_params(self.cfg, kernel, wall)
+        self._tables = []
+        params = make_params(self.cfg, kernel, wall, self._tables)
         h = C.c_void_p()
         err = C.create_string_buffer(256)
         rc = lib().orc_sim_create(self.lattice._h, C.byref(params), C.byref(h), err, 256)

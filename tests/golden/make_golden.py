@@ -2,7 +2,8 @@
 
 Run in a container where the reference is mounted (its path is the first
 argument, default /root/reference).  It copies the reference's own 380-byte
-unit-test geometry (src/unittests/resources/four_cube.gmy) and records, for the
+unit-test geometry (src/unittests/resources/four_cube.gmy) and its file-iolet
+fixtures (iolet.txt, config_file_inlet.xml), and records, for the
 geometries shipped with the reference's example cases, the site counts and
 table checksums that the oracle reads from them.
 """
@@ -30,6 +31,10 @@ def sha(a):
 def main():
     src = os.path.join(REF, "src/unittests/resources/four_cube.gmy")
     shutil.copyfile(src, os.path.join(HERE, "four_cube.gmy"))
+    # The file-pressure iolet fixtures of InOutLetTests::TestFileConstruct
+    # (src/unittests/lbtests/iolets/InOutLetTests.h:117-162).
+    for name in ("iolet.txt", "config_file_inlet.xml"):
+        shutil.copyfile(os.path.join(REF, "src/unittests/resources", name), os.path.join(HERE, name))
     out = {}
     for rel in CASES:
         lat = O.Lattice(os.path.join(REF, rel))

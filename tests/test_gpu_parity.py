@@ -117,3 +117,24 @@ def test_moment_sums_match_distributions(case_dir, precision):
     ref = np.array([f.sum(), (f * cx).sum(), (f * cy).sum(), (f * cz).sum()])
     assert abs(sums[0] - ref[0]) <= 1e-12 * abs(ref[0])
     assert np.max(np.abs(sums[1:] - ref[1:])) <= 1e-12 * abs(ref[0])
+
+
+def test_file_inlet_and_wk2_outlet_bit_exact(tmp_path):
+    """A file-pressure inlet (InOutLetFile) and a two-element Windkessel outlet
+    (InOutLetWK2): FP64 bit-exact with the oracle, the Windkessel state included;
+    the FP32 form within 1e-4."""
+    from test_cpu_iolets import _pipe_case
+    xml, steps = _pipe_case(tmp_path, trailing_newline=True)
+    gpu = lbm.LBM(xml, kernel="LBGK", wall="SBB")
+    orc = O.Simulation(xml, "LBGK", "SBB")
+    gpu.step(steps, macro=True)
+    assert orc.run(steps, macro=True) == 0
+    assert np.array_equal(gpu.GetFOld(), orc.f())
+    rho_g, u_g, w_g = gpu.GetPropertyCache()
+    rho_o, u_o, w_o = orc.macro()
+    assert np.array_equal(rho_g, rho_o) and np.array_equal(u_g, u_o)
+    assert np.array_equal(gpu.GetWK3(1, 0), orc.wk3(1, 0))
+    assert np.max(np.abs(u_o)) > 0
+    f32 = lbm.LBM(xml, kernel="LBGK", wall="SBB", precision="fp32")
+    f32.step(steps, macro=True)
+    assert rel_dev(f32.GetPropertyCache()[1], u_o) <= 1e-4
