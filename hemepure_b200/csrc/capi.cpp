@@ -447,7 +447,7 @@ int hb_read_case(const char* xml_path, int kernel, hb_params* params, char* gmy_
     hb::CaseConfig c = hb::read_case(xml_path, kernel);
     *params = c.params;
     // The file iolets' tables live in `c`: the caller gets them from hb_read_case_iolet_table.
-    for (int k = 0; k < 16; k++) params->inlets[k].density_table = params->outlets[k].density_table = nullptr;
+    for (int k = 0; k < 16; k++) params->inlets[k].table = params->outlets[k].table = nullptr;
     if (gmy_path && gmy_path_len) {
       std::strncpy(gmy_path, c.gmy_path.c_str(), gmy_path_len - 1);
       gmy_path[gmy_path_len - 1] = '\0';
@@ -461,10 +461,15 @@ int hb_read_case_iolet_table(const char* xml_path, int kernel, int outlet, int i
   return guard(nullptr, [&] {
     hb::CaseConfig c = hb::read_case(xml_path, kernel);
     const std::vector<double>& t = c.tables[16 * outlet + index];
-    if (t.empty()) throw hb::Error{HB_ERR_ARG, "that iolet is not a file pressure iolet"};
+    if (t.empty()) throw hb::Error{HB_ERR_ARG, "that iolet is not a file iolet"};
     for (uint64_t k = 0; k < count; k++) out[k] = t[k < t.size() ? k : t.size() - 1];
     return HB_OK;
   });
+}
+
+int hb_iolet_velocity(const hb_iolet* iolet, const double x[3], uint64_t t, double v[3]) {
+  if (!iolet || !x || !v) return HB_ERR_ARG;
+  return guard(nullptr, [&] { return hb::iolet_velocity(*iolet, x, t, v); });
 }
 
 int hb_geometry_open(const char* gmy_path, hb_geometry** out) {

@@ -2,8 +2,12 @@
 //
 // Case file: src/configuration/SimConfig.cc:84-198 (simulation), 262-408 (iolets),
 // 640-655 (iolet position/normal), 668-723 (initial conditions, sponge),
-// 725-754 (cosine), 756-794 (file, WK2), 796-824 (WK3), 856-876 (parabolic); the
-// file iolet's density table src/lb/iolets/InOutLetFile.cc:48-127; unit conversion
+// 725-754 (cosine), 756-794 (file, WK2), 796-824 (WK3), 826-854 (fileWK),
+// 856-876 (parabolic), 878-901 (Womersley), 937-954 (file velocity); the file
+// iolets' tables src/lb/iolets/InOutLetFile.cc:48-127 and
+// InOutLetFileVelocity.cc:34-101; velocity profiles InOutLetParabolicVelocity.cc,
+// InOutLetFileVelocity.cc:104-128, InOutLetWomersleyVelocity.cc:25-41 with
+// src/util/Bessel.cc:17-43; unit conversion
 // src/util/UnitConverter.cc:15-118 and UnitConverter.h:153-203; tau from
 // src/lb/LbmParameters.h:29-37.
 //
@@ -82,6 +86,7 @@ struct Units {
     else if (u == "rad" || u == "dimensionless") sf = 1.;
     else if (u == "m/s") sf = dx / dt;
     else if (u == "mmHg") sf = mass / (dx * dt * dt) / kMmHgToPascal;
+    else if (u == "mmHg/m") sf = mass / (dx * dx * dt * dt) / kMmHgToPascal;
     else throw Error{HB_ERR_FORMAT, "Unknown units '" + u + "'"};
     return v / sf;
   }
@@ -97,10 +102,12 @@ double linear_interpolate(const std::vector<double>& xs, const std::vector<doubl
   return ys[i] + (x - xs[i]) / (xs[i + 1] - xs[i]) * (ys[i + 1] - ys[i]);
 }
 
-// InOutLetFile::CalculateTable: the lattice density at every step 0..total_steps
-// from a file of (time in s, pressure in mmHg) pairs, and the minimum density.
-void file_density_table(const std::string& path, uint64_t total_steps, double dt, const Units& u,
-                        std::vector<double>& table, double& density_min) {
+// The read loop and end-of-run clipping shared by InOutLetFile::CalculateTable
+// (src/lb/iolets/InOutLetFile.cc:48-98) and InOutLetFileVelocity::CalculateTable
+// (src/lb/iolets/InOutLetFileVelocity.cc:34-76): (time in s, value) pairs in
+// time order, cut at total_steps * dt with an interpolated last pair.
+void read_profile(const std::string& path, uint64_t total_steps, double dt, std::vector<double>& times,
+                  std::vector<double>& values) {
   std::ifstream in(path);
   if (!in) throw Error{HB_ERR_IO, "cannot open iolet file " + path};
   std::map<double, double> pairs;
@@ -109,34 +116,54 @@ void file_density_table(const std::string& path, uint64_t total_steps, double dt
     in >> t >> v;
     pairs[t] = v;
   }
-  std::vector<double> times, values;
-  double pmin = pairs.begin()->second, pmax = pmin;
   const double end = (double)total_steps * dt;
   for (const auto& e : pairs) {
     if (e.first > end) {
       if (times.empty()) throw Error{HB_ERR_FORMAT, "file iolet: the file starts after the simulation ends"};
       const double ratio = (end - times.back()) / (e.first - times.back());
-      const double final_p = values.back() + ratio * (e.second - values.back());
+      const double final_v = values.back() + ratio * (e.second - values.back());
       times.push_back(end);
-      pmin = std::min(pmin, final_p);
-      pmax = std::max(pmax, final_p);
-      values.push_back(final_p);
+      values.push_back(final_v);
       break;
     }
-    pmin = std::min(pmin, e.second);
-    pmax = std::max(pmax, e.second);
     times.push_back(e.first);
     values.push_back(e.second);
   }
-  density_min = u.pressure_abs(pmin) / kCs2;
+}
+
+// Both tables loop the file's profile with the same (odd) point formula:
+// point = t_first + ((ts mod steps in the profile) / total_steps) * (t_last - t_first).
+template <class F>
+void profile_table(const std::vector<double>& times, const std::vector<double>& values, uint64_t total_steps,
+                   double dt, std::vector<double>& table, F to_lattice) {
   const int period = (int)(times.back() / dt);
   if (period <= 0 || total_steps == 0) throw Error{HB_ERR_FORMAT, "file iolet: the file spans less than one step"};
   table.resize(total_steps + 1);
   for (uint64_t ts = 0; ts <= total_steps; ts++) {
     const double point =
         times.front() + ((double)(ts % (uint64_t)period) / (double)total_steps) * (times.back() - times.front());
-    table[ts] = u.pressure_abs(linear_interpolate(times, values, point)) / kCs2;
+    table[ts] = to_lattice(linear_interpolate(times, values, point));
   }
+}
+
+// InOutLetFile::CalculateTable: the lattice density at every step 0..total_steps
+// from a file of (time in s, pressure in mmHg) pairs, and the minimum density.
+void file_density_table(const std::string& path, uint64_t total_steps, double dt, const Units& u,
+                        std::vector<double>& table, double& density_min) {
+  std::vector<double> times, values;
+  read_profile(path, total_steps, dt, times, values);
+  density_min = u.pressure_abs(*std::min_element(values.begin(), values.end())) / kCs2;
+  profile_table(times, values, total_steps, dt, table, [&](double p) { return u.pressure_abs(p) / kCs2; });
+}
+
+// InOutLetFileVelocity::CalculateTable: the lattice peak speed at every step
+// 0..total_steps from a file of (time in s, speed in m/s) pairs
+// (UnitConverter::ConvertVelocityToLatticeUnits divides by voxel / time step).
+void file_velocity_table(const std::string& path, uint64_t total_steps, double dt, const Units& u,
+                         std::vector<double>& table) {
+  std::vector<double> times, values;
+  read_profile(path, total_steps, dt, times, values);
+  profile_table(times, values, total_steps, dt, table, [&](double v) { return v / u.speed; });
 }
 
 void normalise(double n[3]) {
@@ -247,8 +274,36 @@ CaseConfig read_case(const std::string& xml_path, int kernel) {
         }
         std::vector<double>& table = c.tables[group_index * 16 + (count - 1)];
         file_density_table(path, c.total_steps, c.dt, u, table, io.density_min);
-        io.density_table = table.data();
+        io.table = table.data();
         io.table_steps = table.size();
+      } else if (type == "pressure" && sub == "fileWK") {
+        // InOutLetFileWK: a WK2 whose weights file is read only in builds with
+        // HEMELB_USE_VELOCITY_WEIGHTS_FILE, and whose radius is never set.
+        io.kind = kWK2;
+        cond.require("path");
+        io.rp = parse_double(dim_value(cond.require("R"), "kg/m^4*s"), "R") * ((c.dt * c.dx) / kBloodDensity);
+        io.cp = parse_double(dim_value(cond.require("C"), "m^4*s^2/kg"), "C") * (kBloodDensity / (c.dt * c.dt * c.dx));
+        io.area = parse_double(dim_value(cond.require("area"), "m^2"), "area") / (c.dx * c.dx);
+      } else if (type == "velocity" && sub == "file") {
+        io.kind = kFileVelocity;
+        std::string path = cond.require("path").attr("value");
+        if (!path.empty() && path[0] != '/') {
+          const size_t slash = xml_path.rfind('/');
+          if (slash != std::string::npos) path = xml_path.substr(0, slash + 1) + path;
+        }
+        io.radius = u.to_lattice("m", parse_double(dim_value(cond.require("radius"), "m"), "radius"));
+        std::vector<double>& table = c.tables[group_index * 16 + (count - 1)];
+        file_velocity_table(path, c.total_steps, c.dt, u, table);
+        io.table = table.data();
+        io.table_steps = table.size();
+      } else if (type == "velocity" && sub == "womersley") {
+        io.kind = kWomersley;
+        io.radius = u.to_lattice("m", parse_double(dim_value(cond.require("radius"), "m"), "radius"));
+        io.pressure_gradient_amplitude = u.to_lattice(
+            "mmHg/m", parse_double(dim_value(cond.require("pressure_gradient_amplitude"), "mmHg/m"), "pressure_gradient_amplitude"));
+        io.period = u.to_lattice("s", parse_double(dim_value(cond.require("period"), "s"), "period"));
+        io.womersley_number = u.to_lattice(
+            "dimensionless", parse_double(dim_value(cond.require("womersley_number"), "dimensionless"), "womersley_number"));
       } else if (type == "velocity" && sub == "parabolic") {
         io.kind = kParabolic;
         io.radius = u.to_lattice("m", parse_double(dim_value(cond.require("radius"), "m"), "radius"));
@@ -273,6 +328,81 @@ CaseConfig read_case(const std::string& xml_path, int kernel) {
     }
   }
   return c;
+}
+
+// ---------------------------------------------------------------------------
+// Velocity iolets on the host
+// ---------------------------------------------------------------------------
+
+// The power series J0(z) = sum_k (-z^2/4)^k / (k!)^2, summed in the order and
+// with the stopping rule of util::BesselJ0ComplexArgument: stop once the last
+// term's squared modulus is at most tol_sq.
+std::complex<double> bessel_j0(const std::complex<double>& z, double tol_sq) {
+  std::complex<double> sum(1.0, 0.0), zpow(1.0, 0.0), term(1.0, 0.0);
+  double fact = 1;
+  for (unsigned k = 1; term.real() * term.real() + term.imag() * term.imag() > tol_sq; ++k) {
+    fact *= k;
+    zpow *= -0.25 * z * z;
+    term = zpow / (fact * fact);
+    sum += term;
+  }
+  return sum;
+}
+
+namespace {
+
+// |x - position|^2 - ((x - position) . normal)^2, in the iolets' order of operations
+// (InOutLetParabolicVelocity.cc:33-36, InOutLetWomersleyVelocity.cc:28-30).
+double radial_sq(const hb_iolet& io, const double x[3]) {
+  const double dx = x[0] - io.position[0], dy = x[1] - io.position[1], dz = x[2] - io.position[2];
+  const double z = dx * io.normal[0] + dy * io.normal[1] + dz * io.normal[2];
+  return (dx * dx + dy * dy + dz * dz) - z * z;
+}
+
+}  // namespace
+
+// InOutLetWomersleyVelocity::GetVelocity (src/lb/iolets/InOutLetWomersleyVelocity.cc:25-41)
+// without its last factor exp(i omega t); the grouping of the products is the
+// reference's, so the host's std::complex arithmetic rounds as it does.
+std::complex<double> womersley_amplitude(const hb_iolet& io, const double x[3]) {
+  const double r = std::sqrt(radial_sq(io, x));
+  const double omega = 2.0 * kPi / io.period;
+  const double density = 1.0;
+  const std::complex<double> i(0, 1);
+  const std::complex<double> i32 = std::pow(i, 1.5);
+  const std::complex<double> numer = bessel_j0(i32 * io.womersley_number * r / io.radius);
+  const std::complex<double> denom = bessel_j0(i32 * io.womersley_number);
+  return io.pressure_gradient_amplitude / (density * omega) * (1.0 - numer / denom);
+}
+
+std::complex<double> womersley_phase(const hb_iolet& io, uint64_t t) {
+  const std::complex<double> i(0, 1);
+  const double omega = 2.0 * kPi / io.period;
+  return std::exp(i * omega * double(t));
+}
+
+int iolet_velocity(const hb_iolet& io, const double x[3], uint64_t t, double v[3]) {
+  if (io.kind == kWomersley) {
+    const double speed = std::real(womersley_amplitude(io, x) * womersley_phase(io, t));
+    for (int k = 0; k < 3; k++) v[k] = io.normal[k] * -speed;
+    return 0;
+  }
+  if (io.kind != kParabolic && io.kind != kFileVelocity) return HB_ERR_UNSUPPORTED;
+  // InOutLetParabolicVelocity::GetVelocity (src/lb/iolets/InOutLetParabolicVelocity.cc:30-58),
+  // InOutLetFileVelocity::GetVelocity (src/lb/iolets/InOutLetFileVelocity.cc:104-128).
+  const double r2a2 = radial_sq(io, x) / (io.radius * io.radius);
+  if (r2a2 > 1.0) return HB_ERR_IOLET_RADIUS;
+  double mx;
+  if (io.kind == kParabolic) {
+    mx = io.max_speed;
+    if (t < io.warmup) mx *= (double)t / (double)io.warmup;
+  } else {
+    if (!io.table || io.table_steps == 0) return HB_ERR_ARG;
+    mx = io.table[t < io.table_steps ? t : io.table_steps - 1];
+  }
+  const double s = mx * (1. - r2a2);
+  for (int k = 0; k < 3; k++) v[k] = io.normal[k] * s;
+  return 0;
 }
 
 // ---------------------------------------------------------------------------

@@ -2,6 +2,7 @@
 // lattice tables of one rank (the reference's geometry::LatticeData).
 #pragma once
 
+#include <complex>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -27,7 +28,7 @@ struct CaseConfig {
     std::vector<std::string> fields;
   };
   std::vector<PropertyOutput> outputs;
-  std::vector<double> tables[32];  // file iolets' density tables (inlets 0-15, outlets 16-31)
+  std::vector<double> tables[32];  // file iolets' tables (inlets 0-15, outlets 16-31)
   std::string checkpoint_file;    // <initialconditions><checkpoint file=...>
   bool has_time = false;          // <initialconditions><time> present
 };
@@ -59,6 +60,18 @@ struct LatticeTables {
     return !w ? (st == 0 ? 0 : (st == 1 ? 2 : 3)) : (st == 0 ? 1 : (st == 1 ? 4 : 5));
   }
 };
+
+// InOutLetVelocity::GetVelocity on the host for the velocity iolets (parabolic,
+// file velocity, Womersley) at lattice position x and 1-based step t.  Returns 0,
+// or HB_ERR_IOLET_RADIUS for a parabolic or file-velocity point outside the radius.
+int iolet_velocity(const hb_iolet& io, const double x[3], uint64_t t, double v[3]);
+// The Womersley profile split into its time-independent factor at x,
+// A(x) = G / (rho omega) (1 - J0(i^(3/2) alpha r / R) / J0(i^(3/2) alpha)), and
+// its phase exp(i omega t); the speed is Re(A exp(i omega t)) along -normal.
+std::complex<double> womersley_amplitude(const hb_iolet& io, const double x[3]);
+std::complex<double> womersley_phase(const hb_iolet& io, uint64_t t);
+// util::BesselJ0ComplexArgument (src/util/Bessel.cc:17-43).
+std::complex<double> bessel_j0(const std::complex<double>& z, double tol_sq = 1e-12);
 
 // GeometryReader::LoadAndDecompose on one rank + LatticeData construction.
 LatticeTables read_gmy(const std::string& path);

@@ -53,6 +53,7 @@ struct GeneralDev {
   const int* io;          // [G] iolet table index or -1
   const int* cpl;         // [G] Windkessel coupling slot or -1
   const int* xyz;         // [3][G] global coordinates
+  const int* wom;         // [G] row of a Womersley iolet site in StepArgs::wom_amp, or -1 (null without one)
 };
 
 struct StepArgs {
@@ -71,13 +72,21 @@ struct StepArgs {
   uint64_t t;             // 1-based time step of this step
   uint64_t lifetime;      // LES sponge lifetime
   const IoletDev* iolets;
-  const double* dens_row; // iolet densities for this step [32]
+  const double* dens_row; // this step's iolet row [kRowStride]: densities, then velocity-iolet values
+  const double* wom_amp;  // [K][18][4] Womersley factor A of link d of Womersley site k:
+                          // (Re, Im) at the half-way point x + c_d / 2, then at x + c_d
   double* cpl_buf;        // Windkessel coupling contributions
   double* rho;            // macroscopic outputs in storage order (or null)
   double* u;              // [3][np]
   double* wss;
   int* status;            // bit 0 unstable, bit 1 iolet radius, bit 2 bad neighbour
 };
+
+// One row of per-step iolet values: the density of iolet idx (inlets 0-15,
+// outlets 16-31) at [idx]; for a file-velocity iolet its peak speed at
+// [kRowA + idx]; for a Womersley iolet Re and Im of exp(i omega t) at
+// [kRowA + idx] and [kRowB + idx].
+constexpr int kRowA = 32, kRowB = 64, kRowStride = 96;
 
 enum StatusBits { kStatusUnstable = 1, kStatusIoletRadius = 2, kStatusBadNeighbour = 4 };
 

@@ -130,6 +130,48 @@ __device__ __forceinline__ bool parabolic(const IoletDev& I, const double x[3], 
   return !(r2a2 > 1.0);
 }
 
+// InOutLetVelocity::GetVelocity of a velocity iolet for link d of general site g:
+// at the Ladd half-way point pos + c_d / 2 (half) or at the neighbour pos + c_d
+// (the GZS extrapolation).  Parabolic: the profile above.  File velocity
+// (src/lb/iolets/InOutLetFileVelocity.cc:104-128): the same profile with the
+// step's peak speed from the iolet row.  Womersley
+// (src/lb/iolets/InOutLetWomersleyVelocity.cc:25-41): Re(A exp(i omega t)) along
+// -normal, A from the link table and exp(i omega t) from the iolet row, the
+// product's real part rounded as the host's complex multiply rounds it.
+// Returns false for a point outside a parabolic profile's radius.
+__device__ __forceinline__ bool link_velocity(const StepArgs& a, const IoletDev& I, int io, int g, int d, bool half,
+                                              const double pos[3], double v[3]) {
+  if (I.kind == kWomersley) {
+    const double* A = a.wom_amp + ((int64_t)__ldg(a.gen.wom + g) * 18 + (d - 1)) * 4 + (half ? 0 : 2);
+    const double re = __ldg(A), im = __ldg(A + 1);
+    const double speed = re * a.dens_row[kRowA + io] - im * a.dens_row[kRowB + io];
+    v[0] = I.nrm[0] * -speed;
+    v[1] = I.nrm[1] * -speed;
+    v[2] = I.nrm[2] * -speed;
+    return true;
+  }
+  double x[3] = {pos[0], pos[1], pos[2]};
+  if (half) {
+    x[0] += 0.5 * cx(d);
+    x[1] += 0.5 * cy(d);
+    x[2] += 0.5 * cz(d);
+  } else {
+    x[0] += cx(d);
+    x[1] += cy(d);
+    x[2] += cz(d);
+  }
+  if (I.kind == kParabolic) return parabolic(I, x, (uint64_t)(unsigned int)a.t, v);
+  const double dx = x[0] - I.pos[0], dy = x[1] - I.pos[1], dz = x[2] - I.pos[2];
+  const double z = dx * I.nrm[0] + dy * I.nrm[1] + dz * I.nrm[2];
+  const double rsq = (dx * dx + dy * dy + dz * dz) - z * z;
+  const double r2a2 = rsq / (I.radius * I.radius);
+  const double s = a.dens_row[kRowA + io] * (1. - r2a2);
+  v[0] = I.nrm[0] * s;
+  v[1] = I.nrm[1] * s;
+  v[2] = I.nrm[2] * s;
+  return !(r2a2 > 1.0);
+}
+
 __device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
 
 // Pre-collision f of a plain bulk site.
@@ -300,14 +342,10 @@ __device__ __forceinline__ void general_site_f64(const StepArgs& a, int g) {
 #pragma unroll
     for (int d = 1; d < Q; d++) {
       if (!((im >> (d - 1)) & 1u)) continue;
-      if (kind == kParabolic) {
+      if (is_velocity_iolet(kind)) {
         // LaddIoletDelegate::StreamLink (src/lb/streamers/LaddIoletDelegate.h:37-86).
-        double hw[3] = {pos[0], pos[1], pos[2]};
-        hw[0] += 0.5 * cx(d);
-        hw[1] += 0.5 * cy(d);
-        hw[2] += 0.5 * cz(d);
         double w[3];
-        if (!parabolic(I, hw, (uint64_t)(unsigned int)a.t, w)) {
+        if (!link_velocity(a, I, io, g, d, true, pos, w)) {
           atomicOr(a.status, kStatusIoletRadius);
           w[0] = w[1] = w[2] = 0.0;
         }
@@ -340,13 +378,12 @@ __device__ __forceinline__ void general_site_f64(const StepArgs& a, int g) {
       if (q < 0.75) {
         if ((im >> (i - 1)) & 1u) {
           const IoletDev& I = a.iolets[io];
-          if (I.kind != kParabolic) {
+          if (!is_velocity_iolet(I.kind)) {
             sbb = true;
           } else {
-            double np3[3] = {(double)__ldg(G.xyz + g) + cx(i), (double)__ldg(G.xyz + G.G + g) + cy(i),
-                             (double)__ldg(G.xyz + 2 * G.G + g) + cz(i)};
+            const double p3[3] = {(double)__ldg(G.xyz + g), (double)__ldg(G.xyz + G.G + g), (double)__ldg(G.xyz + 2 * G.G + g)};
             double nv[3];
-            if (!parabolic(I, np3, (uint64_t)(unsigned int)a.t, nv)) {
+            if (!link_velocity(a, I, io, g, i, false, p3, nv)) {
               atomicOr(a.status, kStatusIoletRadius);
               nv[0] = nv[1] = nv[2] = 0.0;
             }

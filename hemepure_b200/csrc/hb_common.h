@@ -41,7 +41,9 @@ constexpr double kNoValue = 1.7976931348623157e308;  // std::numeric_limits<doub
 
 enum Kernel { kLBGK = 0, kTRT = 1, kLES = 2 };
 enum Wall { kSBB = 0, kBFL = 1, kGZS = 2 };
-enum IoletKind { kCosine = 0, kWK3 = 1, kParabolic = 2, kWK2 = 3, kFile = 4 };
+enum IoletKind { kCosine = 0, kWK3 = 1, kParabolic = 2, kWK2 = 3, kFile = 4, kFileVelocity = 5, kWomersley = 6 };
+// Velocity iolets take the Ladd streamer; the others the Nash zeroth-order pressure streamer.
+HB_HD constexpr bool is_velocity_iolet(int kind) { return kind == kParabolic || kind == kFileVelocity || kind == kWomersley; }
 
 // Host-side error carrying one of the HB_ERR_* codes.
 struct Error {

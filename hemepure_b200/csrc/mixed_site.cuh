@@ -132,6 +132,32 @@ __device__ __forceinline__ bool parabolic_f(const IoletDev& I, const double x[3]
   return !(r2a2 > 1.0);
 }
 
+// The velocity of a velocity iolet's link d of general site gi (parabolic, file
+// velocity or Womersley; half-way point or neighbour as for the FP64 kernels),
+// evaluated in FP64 and narrowed.
+__device__ __forceinline__ bool link_velocity_f(const StepArgs& a, const IoletDev& I, int io, int gi, int d, bool half,
+                                                const double pos[3], float v[3]) {
+  if (I.kind == kWomersley) {
+    const double* A = a.wom_amp + ((int64_t)__ldg(a.gen.wom + gi) * 18 + (d - 1)) * 4 + (half ? 0 : 2);
+    const double speed = __ldg(A) * a.dens_row[kRowA + io] - __ldg(A + 1) * a.dens_row[kRowB + io];
+    v[0] = (float)(I.nrm[0] * -speed);
+    v[1] = (float)(I.nrm[1] * -speed);
+    v[2] = (float)(I.nrm[2] * -speed);
+    return true;
+  }
+  const double h = half ? 0.5 : 1.0;
+  const double x[3] = {pos[0] + h * cx(d), pos[1] + h * cy(d), pos[2] + h * cz(d)};
+  if (I.kind == kParabolic) return parabolic_f(I, x, (uint64_t)(unsigned int)a.t, v);
+  const double dx = x[0] - I.pos[0], dy = x[1] - I.pos[1], dz = x[2] - I.pos[2];
+  const double z = dx * I.nrm[0] + dy * I.nrm[1] + dz * I.nrm[2];
+  const double r2a2 = ((dx * dx + dy * dy + dz * dz) - z * z) / (I.radius * I.radius);
+  const double s = a.dens_row[kRowA + io] * (1. - r2a2);
+  v[0] = (float)(I.nrm[0] * s);
+  v[1] = (float)(I.nrm[1] * s);
+  v[2] = (float)(I.nrm[2] * s);
+  return !(r2a2 > 1.0);
+}
+
 __device__ __forceinline__ void run_offsets(const StepArgs& a, int r, int* off) {
   const int4* o4 = reinterpret_cast<const int4*>(a.run_off) + 5 * r;
 #pragma unroll
@@ -309,10 +335,9 @@ __device__ __forceinline__ void general_site_m(const StepArgs& a, const MixArgs&
     for (int d = 1; d < Q; d++) {
       if (!((im >> (d - 1)) & 1u)) continue;
       float v;
-      if (I.kind == kParabolic) {
-        const double hw[3] = {pos[0] + 0.5 * cx(d), pos[1] + 0.5 * cy(d), pos[2] + 0.5 * cz(d)};
+      if (is_velocity_iolet(I.kind)) {
         float w[3];
-        if (!parabolic_f(I, hw, (uint64_t)(unsigned int)a.t, w)) {
+        if (!link_velocity_f(a, I, io, gi, d, true, pos, w)) {
           atomicOr(a.status, kStatusIoletRadius);
           w[0] = w[1] = w[2] = 0.0f;
         }
@@ -343,13 +368,12 @@ __device__ __forceinline__ void general_site_m(const StepArgs& a, const MixArgs&
       if (q < 0.75f) {
         if ((im >> (i - 1)) & 1u) {
           const IoletDev& I = a.iolets[io];
-          if (I.kind != kParabolic) {
+          if (!is_velocity_iolet(I.kind)) {
             sbb = true;
           } else {
-            const double np3[3] = {(double)__ldg(G.xyz + gi) + cx(i), (double)__ldg(G.xyz + G.G + gi) + cy(i),
-                                   (double)__ldg(G.xyz + 2 * G.G + gi) + cz(i)};
+            const double p3[3] = {(double)__ldg(G.xyz + gi), (double)__ldg(G.xyz + G.G + gi), (double)__ldg(G.xyz + 2 * G.G + gi)};
             float nv[3];
-            if (!parabolic_f(I, np3, (uint64_t)(unsigned int)a.t, nv)) {
+            if (!link_velocity_f(a, I, io, gi, i, false, p3, nv)) {
               atomicOr(a.status, kStatusIoletRadius);
               nv[0] = nv[1] = nv[2] = 0.0f;
             }

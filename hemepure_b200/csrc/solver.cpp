@@ -75,18 +75,20 @@ Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& 
   if (!(p_.tau > 0.5)) throw Error{HB_ERR_ARG, "tau must exceed 1/2"};
   for (int k = 0; k < p_.n_inlets + p_.n_outlets; k++) {
     const hb_iolet& io = k < p_.n_inlets ? p_.inlets[k] : p_.outlets[k - p_.n_inlets];
-    if (io.kind < 0 || io.kind > kFile) throw Error{HB_ERR_ARG, "unknown iolet kind"};
-    if (io.kind == kFile && (!io.density_table || io.table_steps == 0))
-      throw Error{HB_ERR_ARG, "a file iolet needs its density table"};
+    if (io.kind < 0 || io.kind > kWomersley) throw Error{HB_ERR_ARG, "unknown iolet kind"};
+    if ((io.kind == kFile || io.kind == kFileVelocity) && (!io.table || io.table_steps == 0))
+      throw Error{HB_ERR_ARG, "a file iolet needs its table"};
+    if (io.kind == kWomersley && !(io.period > 0.0 && io.radius > 0.0))
+      throw Error{HB_ERR_ARG, "a Womersley iolet needs a positive period and radius"};
   }
-  // The file iolets' density tables are the caller's only for the call: keep copies.
+  // The file iolets' tables are the caller's only for the call: keep copies.
   for (int idx = 0; idx < 32; idx++) {
     const int cnt = idx < 16 ? p_.n_inlets : p_.n_outlets;
     if (idx % 16 >= cnt) continue;
     hb_iolet& io = idx < 16 ? p_.inlets[idx] : p_.outlets[idx - 16];
-    if (io.kind != kFile) continue;
-    tables_[idx].assign(io.density_table, io.density_table + io.table_steps);
-    io.density_table = tables_[idx].data();
+    if (io.kind != kFile && io.kind != kFileVelocity) continue;
+    tables_[idx].assign(io.table, io.table + io.table_steps);
+    io.table = tables_[idx].data();
   }
   if ((opt_.wall == kBFL || opt_.wall == kGZS) && t_.q.empty()) throw Error{HB_ERR_ARG, "BFL and GZS walls need wall distances"};
   check(cudaSetDevice(opt_.device), "cudaSetDevice");
@@ -145,6 +147,41 @@ void Solver::upload() {
   upload_vec(g_io_, L_.g_io, tot);
   upload_vec(g_cpl_, L_.g_cpl, tot);
   upload_vec(g_xyz_, L_.g_xyz, tot);
+  // Womersley links: the time-independent factor of the profile at the two points
+  // a link's velocity is taken at (the Ladd half-way point, and the neighbour the
+  // GZS wall rule extrapolates from), computed once on the host.
+  {
+    std::vector<int> wom(L_.G, -1);
+    std::vector<double> amp;
+    for (int g = 0; g < L_.G; g++) {
+      const uint32_t im = L_.g_iolet[g];
+      if (!im) continue;
+      const int idx = L_.g_io[g];
+      const hb_iolet& c = idx < 16 ? p_.inlets[idx] : p_.outlets[idx - 16];
+      if (c.kind != kWomersley) continue;
+      wom[g] = (int)(amp.size() / (18 * 4));
+      amp.resize(amp.size() + 18 * 4, 0.0);
+      double* row = amp.data() + amp.size() - 18 * 4;
+      const double x0 = L_.g_xyz[g], y0 = L_.g_xyz[(size_t)L_.G + g], z0 = L_.g_xyz[2 * (size_t)L_.G + g];
+      for (int d = 1; d < Q; d++) {
+        if (!((im >> (d - 1)) & 1u)) continue;
+        double hw[3] = {x0, y0, z0};
+        hw[0] += 0.5 * cx(d);
+        hw[1] += 0.5 * cy(d);
+        hw[2] += 0.5 * cz(d);
+        const double nb[3] = {x0 + cx(d), y0 + cy(d), z0 + cz(d)};
+        const std::complex<double> ah = womersley_amplitude(c, hw), an = womersley_amplitude(c, nb);
+        row[(d - 1) * 4 + 0] = ah.real();
+        row[(d - 1) * 4 + 1] = ah.imag();
+        row[(d - 1) * 4 + 2] = an.real();
+        row[(d - 1) * 4 + 3] = an.imag();
+      }
+    }
+    if (!amp.empty()) {
+      upload_vec(g_wom_, wom, tot);
+      upload_vec(wom_amp_, amp, tot);
+    }
+  }
 
   // LES sponge relaxation time per site (LBGKLESSpongeLayer::InitState,
   // src/lb/kernels/LBGKLESSpongeLayer.h:87-116), in storage order.
@@ -213,9 +250,9 @@ void Solver::upload() {
   std::vector<double> zeros(std::max(1, L_.cpl_total), 0.0);
   upload_vec(cpl_buf_, zeros, tot);
   dens_rows_ = 1024;
-  dens_.alloc((size_t)dens_rows_ * 32 * sizeof(double));
+  dens_.alloc((size_t)dens_rows_ * kRowStride * sizeof(double));
   tot += (int64_t)dens_.bytes;
-  host_rows_.assign((size_t)dens_rows_ * 32, 1.0);
+  host_rows_.assign((size_t)dens_rows_ * kRowStride, 1.0);
   status_.alloc(sizeof(int));
   check(cudaMemset(status_.p, 0, sizeof(int)), "cudaMemset");
   dev_bytes_ = tot;
@@ -269,6 +306,8 @@ StepArgs Solver::args() const {
   a.gen.io = g_io_.as<int>();
   a.gen.cpl = g_cpl_.as<int>();
   a.gen.xyz = g_xyz_.as<int>();
+  a.gen.wom = g_wom_.as<int>();
+  a.wom_amp = wom_amp_.as<double>();
   a.tau = p_.tau;
   a.omega = omega_;
   a.omega_minus = omega_minus_;
@@ -276,7 +315,7 @@ StepArgs Solver::args() const {
   a.t = t_step_;
   a.lifetime = p_.sponge_lifetime;
   a.iolets = iolets_.as<IoletDev>();
-  a.dens_row = dens_.as<double>() + (size_t)row_ * 32;
+  a.dens_row = dens_.as<double>() + (size_t)row_ * kRowStride;
   a.cpl_buf = cpl_buf_.as<double>();
   a.rho = rho_.as<double>();
   a.u = u_.as<double>();
@@ -285,8 +324,9 @@ StepArgs Solver::args() const {
   return a;
 }
 
-// Host-side iolet densities for `count` steps from t_first (1-based): the cosine
-// iolets' GetDensity(t - 1).  Windkessel entries are written on the device.
+// Host-side iolet rows for `count` steps from t_first (1-based): the cosine and
+// file iolets' GetDensity(t - 1), the file-velocity iolets' peak speed at t and
+// the Womersley iolets' exp(i omega t).  Windkessel entries are written on the device.
 void Solver::fill_density_rows(uint64_t t_first, int count) {
   double mind = 1.7976931348623157e308;
   for (int k = 0; k < p_.n_inlets + p_.n_outlets; k++) {
@@ -312,15 +352,28 @@ void Solver::fill_density_rows(uint64_t t_first, int count) {
           }
         }
       }
+      double va = 0.0, vb = 0.0;
       if (idx % 16 < cnt) {
         const hb_iolet& c = idx < 16 ? p_.inlets[idx] : p_.outlets[idx - 16];
-        if (c.kind == kFile) v = c.density_table[t0 < c.table_steps ? t0 : c.table_steps - 1];
+        if (c.kind == kFile) v = c.table[t0 < c.table_steps ? t0 : c.table_steps - 1];
+        // Velocity iolets see BoundaryValues::GetTimeStep, the 1-based step as unsigned int.
+        const uint64_t t1 = (uint64_t)(unsigned int)(t0 + 1);
+        if (c.kind == kFileVelocity) va = c.table[t1 < c.table_steps ? t1 : c.table_steps - 1];
+        if (c.kind == kWomersley) {
+          const std::complex<double> e = womersley_phase(c, t1);
+          va = e.real();
+          vb = e.imag();
+        }
       }
-      host_rows_[(size_t)r * 32 + idx] = v;
+      double* row = host_rows_.data() + (size_t)r * kRowStride;
+      row[idx] = v;
+      row[kRowA + idx] = va;
+      row[kRowB + idx] = vb;
     }
   }
-  check(cudaMemcpyAsync(dens_.p, host_rows_.data(), (size_t)count * 32 * sizeof(double), cudaMemcpyHostToDevice, stream_),
-        "density table upload");
+  check(cudaMemcpyAsync(dens_.p, host_rows_.data(), (size_t)count * kRowStride * sizeof(double), cudaMemcpyHostToDevice,
+                        stream_),
+        "iolet row upload");
 }
 
 void Solver::request_comms() {
@@ -328,7 +381,7 @@ void Solver::request_comms() {
     fill_density_rows(t_step_, 1);
     row_ = 0;
   }
-  launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * 32, stream_);
+  launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
   phase_open_ = true;
 }
 
@@ -406,7 +459,7 @@ int Solver::step(int64_t nsteps, uint32_t flags) {
     for (int j = 0; j < chunk; j++) {
       row_ = j;
       phase_open_ = true;
-      launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * 32, stream_);
+      launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
       const bool macro = (flags & HB_STEP_MACRO) && (done + j == nsteps - 1);
       pre_receive(macro);
       end_iteration();
@@ -440,7 +493,7 @@ int Solver::profile(int64_t nsteps, double ms[3]) {
       for (int j = 0; j < chunk; j++) {
         row_ = j;
         phase_open_ = true;
-        launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * 32, stream_);
+        launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
         check(cudaEventRecord(e[0], stream_), "event");
         if (pass == 0) {
           pre_receive(false, 3);

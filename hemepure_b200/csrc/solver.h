@@ -82,7 +82,7 @@ class Solver {
 
   LatticeTables t_;
   hb_params p_;
-  std::vector<double> tables_[32];  // file iolets' density tables (p_ points into them)
+  std::vector<double> tables_[32];  // file iolets' tables (p_ points into them)
   hb_options opt_;
   Layout L_;
   cudaStream_t stream_ = nullptr;
@@ -97,6 +97,7 @@ class Solver {
   DeviceBuffer meta_, run_off_, st2ref_;
   DeviceBuffer g_run_;
   DeviceBuffer g_site_, g_wall_, g_iolet_, g_src_, g_q_, g_nrm_, g_io_, g_cpl_, g_xyz_;
+  DeviceBuffer g_wom_, wom_amp_;     // Womersley link factors (allocated only with such an iolet)
   DeviceBuffer vtau_, iolets_, dens_, cpl_buf_, wk3_, status_;
   DeviceBuffer rho_, u_, wss_;
   DeviceBuffer sum_scratch_, sum_out_;

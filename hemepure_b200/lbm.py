@@ -27,7 +27,7 @@ STATUS_NAMES = {1: "HB_UNSTABLE", -1: "HB_ERR_ARG", -2: "HB_ERR_IO", -3: "HB_ERR
 KERNELS = {"LBGK": 0, "TRT": 1, "LBGKLESSL": 2}
 WALLS = {"SBB": 0, "BFL": 1, "GZS": 2}
 PRECISIONS = {"fp64": 0, "fp32": 1, "fp16": 2}
-IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2, "wk2": 3, "file": 4}
+IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2, "wk2": 3, "file": 4, "file_velocity": 5, "womersley": 6}
 STEP_MACRO = 1
 
 # Every entry point include/hemeb200.h declares.
@@ -42,7 +42,7 @@ EXPORTS = [
     "hb_batch_bytes", "hb_batch_create", "hb_batch_destroy", "hb_batch_add_xml", "hb_batch_add", "hb_batch_remove",
     "hb_batch_run", "hb_batch_get_macro", "hb_batch_member_info", "hb_batch_set_tuning", "hb_batch_stats",
     "hb_batch_prepare_xml", "hb_batch_prep_sites", "hb_batch_add_prepared", "hb_batch_prep_free",
-    "hb_write_xtr_selected", "hb_geometry_select", "hb_read_case_iolet_table",
+    "hb_write_xtr_selected", "hb_geometry_select", "hb_read_case_iolet_table", "hb_iolet_velocity",
 ]
 
 # Extraction geometry selectors (the <geometry type="..."> of a <propertyoutput>).
@@ -69,8 +69,9 @@ class Iolet(C.Structure):
                 ("density_mean", C.c_double), ("density_amp", C.c_double), ("phase", C.c_double),
                 ("period", C.c_double), ("warmup", C.c_uint64), ("radius", C.c_double),
                 ("max_speed", C.c_double), ("rc", C.c_double), ("rp", C.c_double), ("cp", C.c_double),
-                ("area", C.c_double), ("density_table", C.c_void_p),
-                ("table_steps", C.c_uint64), ("density_min", C.c_double)]
+                ("area", C.c_double), ("table", C.c_void_p),
+                ("table_steps", C.c_uint64), ("density_min", C.c_double),
+                ("pressure_gradient_amplitude", C.c_double), ("womersley_number", C.c_double)]
 
 
 class Params(C.Structure):
@@ -138,6 +139,7 @@ def library() -> C.CDLL:
     L.hb_write_xtr_selected.argtypes = [P, C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(Selector)]
     L.hb_geometry_select.argtypes = [P, C.POINTER(Selector), C.c_double, P, P]
     L.hb_read_case_iolet_table.argtypes = [C.c_char_p, I, I, I, P, U64]
+    L.hb_iolet_velocity.argtypes = [C.POINTER(Iolet), P, U64, P]
     L.hb_read_checkpoint.argtypes = [P, C.c_char_p, U64]
     L.hb_last_step_timing.argtypes = [P, P, P]
     L.hb_device_bytes.argtypes = [P, P]
@@ -378,13 +380,27 @@ def read_case(xml_path: str, kernel: str = "LBGK"):
 
 
 def read_case_iolet_table(xml_path: str, kernel: str, outlet: bool, index: int, count: int) -> np.ndarray:
-    """The first `count` entries of a file pressure iolet's density table (no GPU needed)."""
+    """The first `count` entries of a file iolet's table (no GPU needed): lattice
+    densities of a file pressure iolet, peak speeds of a file velocity iolet."""
     out = np.zeros(int(count), np.float64)
     rc = library().hb_read_case_iolet_table(os.fspath(xml_path).encode(), KERNELS[kernel], 1 if outlet else 0,
                                             int(index), _p(out), int(count))
     if rc != HB_OK:
         raise HemeLBError(rc, last_create_error())
     return out
+
+
+def iolet_velocity(iolet: Iolet, x, t: int) -> np.ndarray:
+    """InOutLetVelocity::GetVelocity of a velocity iolet (parabolic, file velocity,
+    Womersley) at lattice position `x` and 1-based step `t`, as the kernels impose
+    it (no GPU needed).  A point outside a parabolic or file profile's radius raises
+    HB_ERR_IOLET_RADIUS, as the reference exits there."""
+    xv = np.ascontiguousarray(x, np.float64)
+    v = np.zeros(3, np.float64)
+    rc = library().hb_iolet_velocity(C.byref(iolet), _p(xv), int(t), _p(v))
+    if rc != HB_OK:
+        raise HemeLBError(rc, "iolet velocity")
+    return v
 
 
 class Geometry:

@@ -457,6 +457,33 @@ class FilePressureBC:
     path: str       # (time in s, pressure in mmHg) pairs, one per line; relative to the case file
 
 
+@dataclass
+class FileWKBC:
+    """InOutLetFileWK: a two-element Windkessel with a weights-file path."""
+    path: str
+    r: float        # lattice units
+    c: float
+    area: float     # lattice units
+
+
+@dataclass
+class FileVelocityBC:
+    """InOutLetFileVelocity: the parabolic profile with a peak speed read from a
+    file of (time in s, speed in m/s) pairs; relative to the case file."""
+    path: str
+    radius: Optional[float] = None     # lattice units; default: the iolet's radius
+
+
+@dataclass
+class WomersleyBC:
+    """InOutLetWomersleyVelocity, in lattice units: pressure-gradient amplitude,
+    period in steps, Womersley number."""
+    pressure_gradient: float
+    period_steps: float
+    womersley_number: float
+    radius: Optional[float] = None
+
+
 def write_case_xml(path: str, gmy_name: str, vessel: Vessel, units: CaseUnits, steps: int,
                    inlet_bcs: Sequence, outlet_bcs: Sequence, warmup: int = 0,
                    relaxation_parameter: Optional[float] = None, sponge: Optional[dict] = None,
@@ -535,6 +562,31 @@ def write_case_xml(path: str, gmy_name: str, vessel: Vessel, units: CaseUnits, s
             elif isinstance(bc, FilePressureBC):
                 L.append('      <condition subtype="file" type="pressure">')
                 L.append(f'        <path value="{bc.path}"/>')
+                L.append('      </condition>')
+            elif isinstance(bc, FileWKBC):
+                res = (units.dt * units.voxel) / BLOOD_DENSITY
+                cap = BLOOD_DENSITY / (units.dt * units.dt * units.voxel)
+                L.append('      <condition subtype="fileWK" type="pressure">')
+                L.append(f'        <path value="{bc.path}"/>')
+                L.append(f'        <R units="kg/m^4*s" value="{bc.r / res!r}"/>')
+                L.append(f'        <C units="m^4*s^2/kg" value="{bc.c / cap!r}"/>')
+                L.append(f'        <area units="m^2" value="{bc.area * units.voxel * units.voxel!r}"/>')
+                L.append('      </condition>')
+            elif isinstance(bc, FileVelocityBC):
+                r = io.radius if bc.radius is None else bc.radius
+                L.append('      <condition subtype="file" type="velocity">')
+                L.append(f'        <path value="{bc.path}"/>')
+                L.append(f'        <radius units="m" value="{float(r) * units.voxel!r}"/>')
+                L.append('      </condition>')
+            elif isinstance(bc, WomersleyBC):
+                r = io.radius if bc.radius is None else bc.radius
+                # mmHg/m -> lattice: divide by mass / (dx^2 dt^2) / mmHg_to_Pa.
+                grad_unit = BLOOD_DENSITY * units.voxel ** 3 / (units.voxel ** 2 * units.dt ** 2) / MMHG_TO_PASCAL
+                L.append('      <condition subtype="womersley" type="velocity">')
+                L.append(f'        <pressure_gradient_amplitude units="mmHg/m" value="{bc.pressure_gradient * grad_unit!r}"/>')
+                L.append(f'        <period units="s" value="{float(bc.period_steps) * units.dt!r}"/>')
+                L.append(f'        <womersley_number units="dimensionless" value="{float(bc.womersley_number)!r}"/>')
+                L.append(f'        <radius units="m" value="{float(r) * units.voxel!r}"/>')
                 L.append('      </condition>')
             else:
                 raise TypeError(bc)

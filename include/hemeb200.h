@@ -36,7 +36,7 @@ extern "C" {
 #define HB_ERR_OOM (-5)          /* device memory exhausted */
 #define HB_ERR_BAD_INDEX (-6)    /* a site or neighbour table failed validation */
 #define HB_ERR_UNSUPPORTED (-7)  /* configuration outside the supported set */
-#define HB_ERR_IOLET_RADIUS (-8) /* parabolic iolet point outside its radius (reference exit(16)) */
+#define HB_ERR_IOLET_RADIUS (-8) /* parabolic or file-velocity iolet point outside its radius (reference exit(16)) */
 #define HB_ERR_TIMEOUT (-9)      /* a bounded device wait gave up */
 
 /* ---- run-time selectable types (reference: compile-time CMake strings,
@@ -54,6 +54,9 @@ extern "C" {
 #define HB_IOLET_PARABOLIC 2     /* Ladd velocity, src/lb/iolets/InOutLetParabolicVelocity.cc */
 #define HB_IOLET_WK2 3           /* Nash pressure, src/lb/iolets/InOutLetWK2.cc (R in rp, C in cp) */
 #define HB_IOLET_FILE 4          /* Nash pressure from a time-pressure file, src/lb/iolets/InOutLetFile.cc */
+#define HB_IOLET_FILE_VELOCITY 5 /* Ladd velocity, parabolic profile whose peak follows a time-speed file,
+                                    src/lb/iolets/InOutLetFileVelocity.cc */
+#define HB_IOLET_WOMERSLEY 6     /* Ladd velocity, Womersley profile, src/lb/iolets/InOutLetWomersleyVelocity.cc */
 
 /* ---- storage precision of the distributions */
 #define HB_STORE_FP64 0          /* plain form: FP64 storage and arithmetic */
@@ -77,17 +80,22 @@ typedef struct hb_iolet {
   int kind;                 /* HB_IOLET_* */
   double position[3];       /* InOutLet::GetPosition */
   double normal[3];         /* normalised; points into the fluid (InOutLet::SetNormal) */
-  double density_mean, density_amp, phase, period; /* cosine (InOutLetCosine) */
+  double density_mean, density_amp, phase, period; /* cosine (InOutLetCosine); period also Womersley */
   uint64_t warmup;          /* extra_warmup_steps */
-  double radius, max_speed; /* parabolic (InOutLetParabolicVelocity) */
-  double rc, rp, cp, area;  /* WK3 (InOutLetWK3); WK2 (InOutLetWK2) uses rp as R and cp as C */
-  /* file pressure (InOutLetFile): lattice density per 0-indexed step (its densityTable;
-   * steps beyond the table take its last entry) and the table's minimum density.  The
-   * library copies the table when a handle is created; hb_read_case leaves it NULL
-   * (hb_read_case_iolet_table fills a caller buffer). */
-  const double* density_table;
+  double radius, max_speed; /* parabolic (InOutLetParabolicVelocity); radius also file velocity, Womersley */
+  double rc, rp, cp, area;  /* WK3 (InOutLetWK3); WK2 and fileWK (InOutLetWK2, InOutLetFileWK) use rp as R, cp as C */
+  /* file iolets: one value per step, indexed as the reference indexes its table (steps
+   * beyond it take its last entry).  File pressure (InOutLetFile): the lattice density
+   * per 0-indexed step (its densityTable), with the table's minimum density.  File
+   * velocity (InOutLetFileVelocity): the lattice peak speed per 1-based step (its
+   * velocityTable).  The library copies the table when a handle is created;
+   * hb_read_case leaves it NULL (hb_read_case_iolet_table fills a caller buffer). */
+  const double* table;
   uint64_t table_steps;
   double density_min;
+  /* Womersley (InOutLetWomersleyVelocity): pressure-gradient amplitude (lattice units),
+   * Womersley number; the period is `period`, the radius `radius`. */
+  double pressure_gradient_amplitude, womersley_number;
 } hb_iolet;
 
 /* LbmParameters + iolet set + initial condition, all in lattice units. */
@@ -277,9 +285,19 @@ int hb_batch_stats(const hb_batch* b, double* last_block_ms, int64_t* active_sit
 /* SimConfig::DoIO for the collide-and-stream path: lattice-unit parameters and
  * the geometry path (resolved against the case file's directory). */
 int hb_read_case(const char* xml_path, int kernel, hb_params* params, char* gmy_path, size_t gmy_path_len);
-/* The density table of a file-pressure iolet of a case (`outlet` 0 for inlets,
- * 1 for outlets; `index` within the group): its first `count` entries. */
+/* The table of a file iolet of a case (`outlet` 0 for inlets, 1 for outlets; `index`
+ * within the group): densities of a file-pressure iolet, peak speeds of a
+ * file-velocity iolet; its first `count` entries. */
 int hb_read_case_iolet_table(const char* xml_path, int kernel, int outlet, int index, double* out, uint64_t count);
+
+/* InOutLetVelocity::GetVelocity of a velocity iolet (parabolic, file velocity or
+ * Womersley) at lattice position x and 1-based time step t, evaluated on the host in
+ * the reference's FP64 arithmetic; the kernels impose exactly these values on the
+ * Ladd links.  A parabolic or file-velocity iolet returns HB_ERR_IOLET_RADIUS for a
+ * point outside its radius (the reference exits there); a pressure iolet returns
+ * HB_ERR_UNSUPPORTED.  Replaces the iolet's own GetVelocity (for example
+ * src/lb/iolets/InOutLetWomersleyVelocity.cc:25-41). */
+int hb_iolet_velocity(const hb_iolet* iolet, const double x[3], uint64_t t, double v[3]);
 
 typedef struct hb_geometry hb_geometry;
 /* GeometryReader + LatticeData on one rank: the reference-order tables. */

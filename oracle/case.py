@@ -7,8 +7,10 @@ other:
 * `src/configuration/SimConfig.cc:84-198` (simulation section, extra warm-up steps),
   `:262-408` (iolets), `:640-655` (iolet position in lattice units, normalised normal),
   `:668-723` (initial conditions, sponge layer), `:725-754` (cosine),
-  `:756-794` (file pressure, WK2), `:796-824` (WK3), `:856-876` (parabolic);
-* `src/lb/iolets/InOutLetFile.cc:48-127` (the file iolet's density table);
+  `:756-794` (file pressure, WK2), `:796-824` (WK3), `:826-854` (fileWK),
+  `:856-876` (parabolic), `:878-901` (Womersley), `:937-954` (file velocity);
+* `src/lb/iolets/InOutLetFile.cc:48-127` (the file pressure iolet's density table),
+  `src/lb/iolets/InOutLetFileVelocity.cc:34-101` (the file velocity iolet's table);
 * `src/util/UnitConverter.cc:15-118`, `src/util/UnitConverter.h:153-203`;
 * `src/lb/LbmParameters.h:29-37` (tau from dt and dx), `src/constants.h`.
 """
@@ -69,6 +71,8 @@ class Units:
             sf = self.dx / self.dt
         elif units == "mmHg":
             sf = self.mass / (self.dx * self.dt * self.dt) / MMHG_TO_PASCAL
+        elif units == "mmHg/m":
+            sf = self.mass / (self.dx * self.dx * self.dt * self.dt) / MMHG_TO_PASCAL
         else:
             raise ValueError(units)
         return value / sf
@@ -85,7 +89,7 @@ class Units:
 
 @dataclass
 class IoletCfg:
-    kind: str                  # "cosine", "wk3", "parabolic"
+    kind: str                  # a key of oracle.IOLET_KINDS
     position: List[float]
     normal: List[float]
     density_mean: float = 0.0
@@ -99,8 +103,10 @@ class IoletCfg:
     rp: float = 0.0
     cp: float = 0.0
     area: float = 0.0
-    table: Optional[List[float]] = None   # file pressure: density per 0-indexed step
-    density_min: float = 0.0
+    table: Optional[List[float]] = None   # file pressure: density per 0-indexed step;
+    density_min: float = 0.0              # file velocity: peak speed per 1-based step
+    pressure_gradient_amplitude: float = 0.0   # Womersley
+    womersley_number: float = 0.0
 
 
 @dataclass
@@ -171,6 +177,32 @@ def file_density_table(path: str, total_steps: int, dt: float, u: "Units"):
         point = times[0] + (float(step % period_steps) / float(total_steps)) * (times[-1] - times[0])
         table.append(u.pressure_to_lattice(_linear_interpolate(times, values, point)) / CS2)
     return table, density_min
+
+
+def file_velocity_table(path: str, total_steps: int, dt: float, u: "Units"):
+    """InOutLetFileVelocity::CalculateTable (src/lb/iolets/InOutLetFileVelocity.cc:34-101):
+    the lattice peak speed at every step 0..total_steps, the file's (time in s,
+    speed in m/s) profile clipped at the run's end and looped like the pressure
+    table."""
+    pairs = _read_time_value_pairs(path)
+    times, values = [], []
+    end = total_steps * dt
+    for t, v in sorted(pairs.items()):
+        if t > end:
+            ratio = (end - times[-1]) / (t - times[-1])
+            times.append(end)
+            values.append(values[-1] + ratio * (v - values[-1]))
+            break
+        times.append(t)
+        values.append(v)
+    period_steps = int(times[-1] / dt)
+    if period_steps <= 0:
+        raise ValueError("the file's time range is shorter than one step")
+    table = []
+    for step in range(total_steps + 1):
+        point = times[0] + (float(step % period_steps) / float(total_steps)) * (times[-1] - times[0])
+        table.append(_linear_interpolate(times, values, point) / u.speed)
+    return table
 
 
 def _normalised(v):
@@ -252,6 +284,28 @@ def load_case(xml_path: str, kernel: str = "LBGK") -> CaseCfg:
                 path = cond.find("path").get("value")
                 path = os.path.normpath(os.path.join(os.path.dirname(os.path.abspath(xml_path)), path))
                 io.table, io.density_min = file_density_table(path, steps, dt, u)
+            elif typ == "pressure" and sub == "fileWK":
+                # InOutLetFileWK behaves as WK2: its weights file is read only in
+                # builds with HEMELB_USE_VELOCITY_WEIGHTS_FILE; its radius is unset.
+                io = IoletCfg("wk2", pos, nrm)
+                if cond.find("path") is None:
+                    raise ValueError("fileWK condition without <path>")
+                io.rp = u.resistance(_val(cond.find("R"), "kg/m^4*s"))
+                io.cp = u.capacitance(_val(cond.find("C"), "m^4*s^2/kg"))
+                io.area = u.area(_val(cond.find("area"), "m^2"))
+            elif typ == "velocity" and sub == "file":
+                io = IoletCfg("file_velocity", pos, nrm)
+                path = cond.find("path").get("value")
+                path = os.path.normpath(os.path.join(os.path.dirname(os.path.abspath(xml_path)), path))
+                io.radius = u.to_lattice("m", _val(cond.find("radius"), "m"))
+                io.table = file_velocity_table(path, steps, dt, u)
+            elif typ == "velocity" and sub == "womersley":
+                io = IoletCfg("womersley", pos, nrm)
+                io.radius = u.to_lattice("m", _val(cond.find("radius"), "m"))
+                io.pressure_gradient_amplitude = u.to_lattice(
+                    "mmHg/m", _val(cond.find("pressure_gradient_amplitude"), "mmHg/m"))
+                io.period = u.to_lattice("s", _val(cond.find("period"), "s"))
+                io.womersley_number = u.to_lattice("dimensionless", _val(cond.find("womersley_number"), "dimensionless"))
             elif typ == "velocity" and sub == "parabolic":
                 io = IoletCfg("parabolic", pos, nrm)
                 io.radius = u.to_lattice("m", _val(cond.find("radius"), "m"))

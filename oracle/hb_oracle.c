@@ -24,12 +24,15 @@
  *   step phases      src/lb/lb.hpp:205-346
  *   iolets           src/lb/iolets/InOutLetCosine.cc:37-54,
  *                    InOutLetParabolicVelocity.cc:30-58, InOutLetWK3.cc:33-105,
+ *                    InOutLetFileVelocity.cc:104-128,
+ *                    InOutLetWomersleyVelocity.cc:15-41, src/util/Bessel.cc:17-43,
  *                    BoundaryValues.cc:20-224, BoundaryComms.cc:48-80
  *   macroscopic      src/lb/streamers/BaseStreamer.h:87-225,
  *                    src/lb/lattices/Lattice.h:1122-1156, 1353-1383
  */
 #include "hb_oracle.h"
 
+#include <complex.h>
 #include <float.h>
 #include <math.h>
 #include <stdio.h>
@@ -564,6 +567,88 @@ static int parabolic_velocity(const iolet_t* io, const double x[3], uint64_t t1,
   return 0;
 }
 
+/* InOutLetFileVelocity::GetVelocity: the parabolic profile with the peak speed
+ * velocityTable[t] (steps past the table take its last entry). */
+static int file_velocity(const iolet_t* io, const double x[3], uint64_t t1, double v[3]) {
+  const double dx = x[0] - io->cfg.position[0], dy = x[1] - io->cfg.position[1], dz = x[2] - io->cfg.position[2];
+  const double* n = io->cfg.normal;
+  const double z = dx * n[0] + dy * n[1] + dz * n[2];
+  const double rsq = (dx * dx + dy * dy + dz * dz) - z * z;
+  const double r2a2 = rsq / (io->cfg.radius * io->cfg.radius);
+  if (r2a2 > 1.0) return -1;
+  const double mx = io->cfg.table[t1 < io->cfg.table_len ? t1 : io->cfg.table_len - 1];
+  const double s = mx * (1. - r2a2);
+  v[0] = n[0] * s;
+  v[1] = n[1] * s;
+  v[2] = n[2] * s;
+  return 0;
+}
+
+/* util::BesselJ0ComplexArgument: the power series of J0, summed until the squared
+ * modulus of the last term is at most tol_sq, in the reference's operation order. */
+static double complex bessel_j0(double complex z, double tol_sq) {
+  double complex sum = 1.0, zpow = 1.0, term = 1.0;
+  double fact = 1;
+  for (unsigned k = 1; creal(term) * creal(term) + cimag(term) * cimag(term) > tol_sq; ++k) {
+    fact *= k;
+    zpow *= -0.25 * z * z;
+    term = zpow / (fact * fact);
+    sum += term;
+  }
+  return sum;
+}
+
+void orc_bessel_j0(double re, double im, double out[2]) {
+  const double complex j = bessel_j0(CMPLX(re, im), 1e-12);
+  out[0] = creal(j);
+  out[1] = cimag(j);
+}
+
+/* InOutLetWomersleyVelocity::GetVelocity:
+ *   v = -normal Re[ G / (rho omega) (1 - J0(i^(3/2) alpha r / R) / J0(i^(3/2) alpha)) exp(i omega t) ]
+ * with rho = 1.  i^(3/2) is std::pow(complex i, 1.5) of the C++ library the
+ * reference builds with: polar(exp(1.5 Re log i), 1.5 Im log i). */
+static void womersley_velocity(const iolet_t* io, const double x[3], uint64_t t1, double v[3]) {
+  const double dx = x[0] - io->cfg.position[0], dy = x[1] - io->cfg.position[1], dz = x[2] - io->cfg.position[2];
+  const double* n = io->cfg.normal;
+  const double z = dx * n[0] + dy * n[1] + dz * n[2];
+  const double r = sqrt((dx * dx + dy * dy + dz * dz) - z * z);
+  const double omega = 2.0 * PI_ / io->cfg.period;
+  const double density = 1.0;
+  const double complex lg = clog(CMPLX(0.0, 1.0));
+  const double rho = exp(1.5 * creal(lg)), th = 1.5 * cimag(lg);
+  const double complex i32 = CMPLX(rho * cos(th), rho * sin(th));
+  const double complex numer = bessel_j0(i32 * io->cfg.womersley_number * r / io->cfg.radius, 1e-12);
+  const double complex denom = bessel_j0(i32 * io->cfg.womersley_number, 1e-12);
+  const double complex amp = io->cfg.pressure_gradient_amplitude / (density * omega) * (1.0 - numer / denom);
+  const double speed = creal(amp * cexp(CMPLX(0.0, omega * (double)t1)));
+  v[0] = n[0] * -speed;
+  v[1] = n[1] * -speed;
+  v[2] = n[2] * -speed;
+}
+
+static int is_velocity_iolet(const iolet_t* io) {
+  return io->cfg.kind == ORC_IOLET_PARABOLIC || io->cfg.kind == ORC_IOLET_FILE_VELOCITY || io->cfg.kind == ORC_IOLET_WOMERSLEY;
+}
+
+/* The velocity iolets' GetVelocity; 0, or -1 outside a parabolic profile's radius. */
+static int iolet_velocity(const iolet_t* io, const double x[3], uint64_t t1, double v[3]) {
+  if (io->cfg.kind == ORC_IOLET_WOMERSLEY) {
+    womersley_velocity(io, x, t1, v);
+    return 0;
+  }
+  if (io->cfg.kind == ORC_IOLET_FILE_VELOCITY) return file_velocity(io, x, t1, v);
+  return parabolic_velocity(io, x, t1, v);
+}
+
+int orc_iolet_velocity(const orc_iolet* cfg, const double x[3], uint64_t t, double v[3]) {
+  iolet_t io;
+  memset(&io, 0, sizeof(io));
+  io.cfg = *cfg;
+  if (!is_velocity_iolet(&io)) return -2;
+  return iolet_velocity(&io, x, t, v);
+}
+
 static void sort_dirs_close_to_normal(iolet_t* io) {
   /* Nash/Ladd SortDirectionsCloseToIOletNormal: the direction minimising
    * |c_k/|c_k| - n|^2 (the zero vector stays zero when normalised). */
@@ -824,13 +909,13 @@ static int gzs_link(const orc_sim* s, int64_t i, const hydro_t* h, int ip, doubl
     if (has_iolet(l, i, ii)) {
       const int grp = l->stype[i] == 1 ? 0 : 1;
       const iolet_t* io = &s->io[grp][l->iolet_id[i]];
-      if (io->cfg.kind != ORC_IOLET_PARABOLIC) {
+      if (!is_velocity_iolet(io)) {
         fnew_site[ii] = h->fpost[ip];
         return 0;
       }
       double np[3] = {(double)l->coords[3 * i] + CX[ii], (double)l->coords[3 * i + 1] + CY[ii], (double)l->coords[3 * i + 2] + CZ[ii]};
       double nv[3];
-      if (parabolic_velocity(io, np, (uint64_t)(unsigned int)s->t, nv)) return -1;
+      if (iolet_velocity(io, np, (uint64_t)(unsigned int)s->t, nv)) return -1;
       for (int c = 0; c < 3; c++) {
         const double v2 = nv[c] * (q - 1) / (q + 1);
         mw[c] = q * mw[c] + (1. - q) * h->rho * v2;
@@ -886,14 +971,14 @@ static int site_update(orc_sim* s, int64_t i, int want_macro) {
         s->cpl_u[3 * i + 1] = h.uy;
         s->cpl_u[3 * i + 2] = h.uz;
       }
-      if (io->cfg.kind == ORC_IOLET_PARABOLIC) {
+      if (is_velocity_iolet(io)) {
         /* Ladd: bounce-back minus 2 w rho (u_w . c)/cs^2 at the link half-way point. */
         double hw[3] = {(double)l->coords[3 * i], (double)l->coords[3 * i + 1], (double)l->coords[3 * i + 2]};
         hw[0] += 0.5 * CX[d];
         hw[1] += 0.5 * CY[d];
         hw[2] += 0.5 * CZ[d];
         double wm[3];
-        if (parabolic_velocity(io, hw, (uint64_t)(unsigned int)s->t, wm)) {
+        if (iolet_velocity(io, hw, (uint64_t)(unsigned int)s->t, wm)) {
           rc = -1;
           wm[0] = wm[1] = wm[2] = 0.0;
         }

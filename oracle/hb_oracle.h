@@ -23,7 +23,8 @@ enum { ORC_LBGK = 0, ORC_TRT = 1, ORC_LBGKLES = 2 };
 /* Wall streamers (SimpleBounceBackDelegate.h, BouzidiFirdaousLallemandDelegate.h, GuoZhengShiDelegate.h). */
 enum { ORC_SBB = 0, ORC_BFL = 1, ORC_GZS = 2 };
 /* Iolet streamers and iolet value sources. */
-enum { ORC_IOLET_COSINE = 0, ORC_IOLET_WK3 = 1, ORC_IOLET_PARABOLIC = 2, ORC_IOLET_WK2 = 3, ORC_IOLET_FILE = 4 };
+enum { ORC_IOLET_COSINE = 0, ORC_IOLET_WK3 = 1, ORC_IOLET_PARABOLIC = 2, ORC_IOLET_WK2 = 3, ORC_IOLET_FILE = 4,
+       ORC_IOLET_FILE_VELOCITY = 5, ORC_IOLET_WOMERSLEY = 6 };
 
 typedef struct orc_iolet {
   int kind;                 /* ORC_IOLET_* */
@@ -36,10 +37,13 @@ typedef struct orc_iolet {
   double radius, max_speed;
   /* WK3 (lattice units); WK2 uses rp as its R and cp as its C */
   double rc, rp, cp, area;
-  /* file pressure: density per 0-indexed step (InOutLetFile densityTable) and its minimum */
+  /* file pressure: density per 0-indexed step (InOutLetFile densityTable) and its minimum;
+   * file velocity: peak speed per 1-based step (InOutLetFileVelocity velocityTable) */
   const double* table;
   uint64_t table_len;
   double density_min;
+  /* Womersley: pressure-gradient amplitude and Womersley number (period, radius above) */
+  double pressure_gradient_amplitude, womersley_number;
 } orc_iolet;
 
 typedef struct orc_params {
@@ -90,6 +94,12 @@ void orc_sim_get_macro(const orc_sim* s, double* rho, double* u, double* wss);
 /* WK3 state of iolet `index` of `group` (0 inlets, 1 outlets):
  * density, densityNew, flowRate, flowRateOld. */
 void orc_sim_get_wk3(const orc_sim* s, int group, int index, double st[4]);
+/* InOutLetVelocity::GetVelocity of a velocity iolet (parabolic, file velocity,
+ * Womersley) at lattice position x and 1-based step t.  Returns 0, or -1 for a
+ * point outside a parabolic or file profile's radius, -2 for a pressure iolet. */
+int orc_iolet_velocity(const orc_iolet* io, const double x[3], uint64_t t, double v[3]);
+/* util::BesselJ0ComplexArgument with tolSq = 1e-12 (src/util/Bessel.cc:17-43). */
+void orc_bessel_j0(double re, double im, double out[2]);
 /* Per-site relaxation time of the LES kernel's sponge layer (vTau). */
 void orc_sim_get_vtau(const orc_sim* s, double* vtau);
 

@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "_build", "libhboracle.so")
 
 KERNELS = {"LBGK": 0, "TRT": 1, "LBGKLESSL": 2}
 WALLS = {"SBB": 0, "BFL": 1, "GZS": 2}
-IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2, "wk2": 3, "file": 4}
+IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2, "wk2": 3, "file": 4, "file_velocity": 5, "womersley": 6}
 
 
 def build(force: bool = False) -> str:
@@ -43,7 +43,8 @@ class _Iolet(C.Structure):
                 ("density_mean", C.c_double), ("density_amp", C.c_double), ("phase", C.c_double),
                 ("period", C.c_double), ("warmup", C.c_uint64), ("radius", C.c_double),
                 ("max_speed", C.c_double), ("rc", C.c_double), ("rp", C.c_double), ("cp", C.c_double),
-                ("area", C.c_double), ("table", C.c_void_p), ("table_len", C.c_uint64), ("density_min", C.c_double)]
+                ("area", C.c_double), ("table", C.c_void_p), ("table_len", C.c_uint64), ("density_min", C.c_double),
+                ("pressure_gradient_amplitude", C.c_double), ("womersley_number", C.c_double)]
 
 
 class _Params(C.Structure):
@@ -84,6 +85,8 @@ def lib():
         L.orc_sim_get_macro.argtypes = [P, P, P, P]
         L.orc_sim_get_wk3.argtypes = [P, C.c_int, C.c_int, P]
         L.orc_sim_get_vtau.argtypes = [P, P]
+        L.orc_iolet_velocity.argtypes = [C.POINTER(_Iolet), P, C.c_uint64, P]
+        L.orc_bessel_j0.argtypes = [C.c_double, C.c_double, P]
         _lib = L
     return _lib
 
@@ -167,6 +170,7 @@ def make_params(cfg: case_mod.CaseCfg, kernel: str, wall: str, keep: Optional[li
             d.warmup = io.warmup
             d.radius, d.max_speed = io.radius, io.max_speed
             d.rc, d.rp, d.cp, d.area = io.rc, io.rp, io.cp, io.area
+            d.pressure_gradient_amplitude, d.womersley_number = io.pressure_gradient_amplitude, io.womersley_number
             if io.table is not None:
                 tab = np.ascontiguousarray(io.table, dtype=np.float64)
                 if keep is not None:
@@ -177,6 +181,34 @@ def make_params(cfg: case_mod.CaseCfg, kernel: str, wall: str, keep: Optional[li
     p.n_inlets = len(cfg.inlets)
     p.n_outlets = len(cfg.outlets)
     return p
+
+
+def iolet_params(cfg: case_mod.IoletCfg, keep: list) -> _Iolet:
+    """One iolet's oracle parameter block (its table appended to `keep`)."""
+    c = case_mod.CaseCfg(gmy_path="", tau=1.0, total_steps=0, warmup=0, initial_density=1.0, initial_step=1,
+                         relaxation_parameter=0.0, viscosity_ratio=0.0, sponge_width=0.0, sponge_lifetime=0,
+                         inlets=[cfg])
+    p = make_params(c, "LBGK", "SBB", keep)
+    return p.inlets[0]
+
+
+def iolet_velocity(cfg: case_mod.IoletCfg, x, t: int) -> np.ndarray:
+    """The oracle's InOutLetVelocity::GetVelocity (raises ValueError outside the radius)."""
+    keep = []
+    io = iolet_params(cfg, keep)
+    xv = np.ascontiguousarray(x, np.float64)
+    v = np.zeros(3, np.float64)
+    rc = lib().orc_iolet_velocity(C.byref(io), _ptr(xv), int(t), _ptr(v))
+    if rc != 0:
+        raise ValueError(f"orc_iolet_velocity: {rc}")
+    return v
+
+
+def bessel_j0(z: complex) -> complex:
+    """util::BesselJ0ComplexArgument (tolSq 1e-12) as the oracle restates it."""
+    out = np.zeros(2, np.float64)
+    lib().orc_bessel_j0(float(z.real), float(z.imag), _ptr(out))
+    return complex(out[0], out[1])
 
 
 class Simulation:

@@ -2,8 +2,11 @@
 
 Run in a container where the reference is mounted (its path is the first
 argument, default /root/reference).  It copies the reference's own 380-byte
-unit-test geometry (src/unittests/resources/four_cube.gmy) and its file-iolet
-fixtures (iolet.txt, config_file_inlet.xml), and records, for the
+unit-test geometry (src/unittests/resources/four_cube.gmy), its iolet fixtures
+(iolet.txt, config_file_inlet.xml, velocity_inlet.txt,
+config_file_velocity_inlet.xml, config_new_velocity_inlets.xml), the table of
+J0(i^(3/2) x) that its Bessel unit test holds (bessel_j0_table.json, parsed
+from src/unittests/util/BesselTests.h), and records, for the
 geometries shipped with the reference's example cases, the site counts and
 table checksums that the oracle reads from them.
 """
@@ -11,6 +14,7 @@ table checksums that the oracle reads from them.
 import hashlib
 import json
 import os
+import re
 import shutil
 import sys
 
@@ -33,8 +37,20 @@ def main():
     shutil.copyfile(src, os.path.join(HERE, "four_cube.gmy"))
     # The file-pressure iolet fixtures of InOutLetTests::TestFileConstruct
     # (src/unittests/lbtests/iolets/InOutLetTests.h:117-162).
-    for name in ("iolet.txt", "config_file_inlet.xml"):
+    # The velocity iolet fixtures of InOutLetTests::TestWomersleyVelocityConstruct and
+    # TestFileVelocityConstruct (InOutLetTests.h:200-332).
+    for name in ("iolet.txt", "config_file_inlet.xml", "velocity_inlet.txt", "config_file_velocity_inlet.xml",
+                 "config_new_velocity_inlets.xml"):
         shutil.copyfile(os.path.join(REF, "src/unittests/resources", name), os.path.join(HERE, name))
+    # BesselTests::TestUsedRange (src/unittests/util/BesselTests.h): J0(i^(3/2) x) for
+    # x = 0, 0.1, ..., 20, compared there at an absolute 1e-6.
+    text = open(os.path.join(REF, "src/unittests/util/BesselTests.h")).read()
+    table = text[text.index("mathematica[] = {"):]
+    table = table[:table.index("};")]
+    vals = [(float(a), float(b)) for a, b in re.findall(r"Complex\(\s*([-+0-9.eE]+)\s*,\s*([-+0-9.eE]+)\s*\)", table)]
+    assert len(vals) == 201
+    with open(os.path.join(HERE, "bessel_j0_table.json"), "w") as fh:
+        json.dump({"x": [k / 10.0 for k in range(201)], "j0": vals, "abs_tol": 1e-6}, fh)
     out = {}
     for rel in CASES:
         lat = O.Lattice(os.path.join(REF, rel))

@@ -138,3 +138,28 @@ def test_file_inlet_and_wk2_outlet_bit_exact(tmp_path):
     f32 = lbm.LBM(xml, kernel="LBGK", wall="SBB", precision="fp32")
     f32.step(steps, macro=True)
     assert rel_dev(f32.GetPropertyCache()[1], u_o) <= 1e-4
+
+
+@pytest.mark.parametrize("inlet,kernel,wall", [("womersley", "LBGK", "SBB"), ("womersley", "TRT", "GZS"),
+                                               ("file", "LBGK", "BFL"), ("file", "TRT", "GZS")])
+def test_velocity_inlets_bit_exact(tmp_path, inlet, kernel, wall):
+    """Womersley (InOutLetWomersleyVelocity) into a fileWK outlet, and file velocity
+    (InOutLetFileVelocity) into a pressure outlet, under the Ladd rule, with the GZS
+    walls' extrapolation from a velocity iolet: FP64 bit-exact with the oracle (the
+    Windkessel state included); the FP32 form within 1e-4."""
+    from test_cpu_velocity_iolets import velocity_pipe_case
+    xml, steps = velocity_pipe_case(tmp_path, inlet, relaxation_parameter=3.0 / 16.0 if kernel == "TRT" else None)
+    gpu = lbm.LBM(xml, kernel=kernel, wall=wall)
+    orc = O.Simulation(xml, kernel, wall)
+    gpu.step(steps, macro=True)
+    assert orc.run(steps, macro=True) == 0
+    assert np.array_equal(gpu.GetFOld(), orc.f())
+    rho_g, u_g, w_g = gpu.GetPropertyCache()
+    rho_o, u_o, w_o = orc.macro()
+    assert np.array_equal(rho_g, rho_o) and np.array_equal(u_g, u_o) and np.array_equal(w_g, w_o)
+    if inlet == "womersley":
+        assert np.array_equal(gpu.GetWK3(1, 0), orc.wk3(1, 0))
+    assert np.max(np.abs(u_o)) > 1e-3
+    f32 = lbm.LBM(xml, kernel=kernel, wall=wall, precision="fp32")
+    f32.step(steps, macro=True)
+    assert rel_dev(f32.GetPropertyCache()[1], u_o) <= 1e-4
