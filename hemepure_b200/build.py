@@ -25,6 +25,7 @@ CU_SOURCES = {
     "kernels_mixed.cu": [],
     "noalloc.cu": [],
     "kernels_batch.cu": [],
+    "gmy_device.cu": [],
 }
 CPP_SOURCES = ["xml.cpp", "config.cpp", "layout.cpp", "solver.cpp", "extraction.cpp", "batch.cpp", "capi.cpp"]
 HEADERS = ["hb_common.h", "f64_site.cuh", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h", "mixed_site.cuh", "batch.h", "batch_dev.h"]

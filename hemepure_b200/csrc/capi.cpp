@@ -1,5 +1,6 @@
 // capi.cpp -- the extern "C" boundary (include/hemeb200.h).  No C++ exception
 // crosses it: every entry point catches and returns an HB_* status.
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -17,6 +18,7 @@ struct hb_handle {
 
 struct hb_geometry {
   hb::LatticeTables tables;
+  hb::GmyTiming timing;
 };
 
 struct hb_batch {
@@ -68,6 +70,7 @@ void hb_default_options(hb_options* opt) {
   opt->wall = HB_WALL_SBB;
   opt->precision = HB_STORE_FP64;
   opt->device = 0;
+  opt->geometry_reader = HB_GEOMETRY_DEVICE;
 }
 
 int hb_create_from_xml(const char* xml_path, const hb_options* opt, hb_handle** out) {
@@ -78,7 +81,8 @@ int hb_create_from_xml(const char* xml_path, const hb_options* opt, hb_handle** 
     hb_default_options(&o);
     if (opt) o = *opt;
     hb::CaseConfig c = hb::read_case(xml_path, o.kernel);
-    hb::LatticeTables t = hb::read_gmy(c.gmy_path);
+    hb::LatticeTables t = o.geometry_reader == HB_GEOMETRY_DEVICE ? hb::read_gmy_device(c.gmy_path, o.device)
+                                                                   : hb::read_gmy(c.gmy_path);
     int rc = finish_create(std::move(t), c.params, o, out);
     if (rc == HB_OK) (*out)->solver->set_units(c.dt, c.dx, c.origin);
     if (rc == HB_OK && !c.checkpoint_file.empty()) {
@@ -120,13 +124,9 @@ int hb_create(const hb_lattice_desc* lat, const hb_params* params, const hb_opti
     t.iolet_id.assign(lat->iolet_id, lat->iolet_id + n);
     if (lat->wall_distance) t.q.assign(lat->wall_distance, lat->wall_distance + 18 * n);
     if (lat->wall_normal) t.normal.assign(lat->wall_normal, lat->wall_normal + 3 * n);
-    else t.normal.assign(3 * n, 0.0);
+    else t.normal.assign(3 * n, 0.0f);
     for (int64_t i = 0; i < n; i++) t.type_counts[t.collision_type(i)]++;
-    if (lat->neighbours) {
-      t.nbr.assign(lat->neighbours, lat->neighbours + 19 * n);
-    } else {
-      hb::build_neighbours(t);
-    }
+    if (lat->neighbours) t.nbr.assign(lat->neighbours, lat->neighbours + 19 * n);
     return finish_create(std::move(t), *params, o, out);
   });
 }
@@ -248,16 +248,18 @@ int hb_get_wk3(hb_handle* h, int group, int index, double state[4]) {
 int hb_get_tables(const hb_handle* h, int64_t* neighbours, uint32_t* wall_mask, uint32_t* iolet_mask, int32_t* site_type,
                   int32_t* iolet_id, int64_t* coords, int64_t* type_counts) {
   if (!h) return HB_ERR_ARG;
-  const hb::LatticeTables& t = h->solver->tables();
-  const size_t n = (size_t)t.n;
-  if (neighbours) std::memcpy(neighbours, t.nbr.data(), n * 19 * sizeof(int64_t));
-  if (wall_mask) std::memcpy(wall_mask, t.wall.data(), n * sizeof(uint32_t));
-  if (iolet_mask) std::memcpy(iolet_mask, t.iolet.data(), n * sizeof(uint32_t));
-  if (site_type) std::memcpy(site_type, t.stype.data(), n * sizeof(int32_t));
-  if (iolet_id) std::memcpy(iolet_id, t.iolet_id.data(), n * sizeof(int32_t));
-  if (coords) std::memcpy(coords, t.coords.data(), n * 3 * sizeof(int64_t));
-  if (type_counts) std::memcpy(type_counts, t.type_counts, 6 * sizeof(int64_t));
-  return HB_OK;
+  return guard(nullptr, [&] {
+    const hb::LatticeTables& t = h->solver->tables();
+    const size_t n = (size_t)t.n;
+    if (neighbours) hb::neighbour_table(t, neighbours);
+    if (wall_mask) std::memcpy(wall_mask, t.wall.data(), n * sizeof(uint32_t));
+    if (iolet_mask) std::memcpy(iolet_mask, t.iolet.data(), n * sizeof(uint32_t));
+    if (site_type) std::memcpy(site_type, t.stype.data(), n * sizeof(int32_t));
+    if (iolet_id) std::memcpy(iolet_id, t.iolet_id.data(), n * sizeof(int32_t));
+    if (coords) std::memcpy(coords, t.coords.data(), n * 3 * sizeof(int64_t));
+    if (type_counts) std::memcpy(type_counts, t.type_counts, 6 * sizeof(int64_t));
+    return HB_OK;
+  });
 }
 
 int hb_write_xtr(hb_handle* h, const char* path, const char* fields, const char* offset_path) {
@@ -299,10 +301,9 @@ hb::LatticeTables tables_from_desc(const hb_lattice_desc* lat) {
   t.iolet_id.assign(lat->iolet_id, lat->iolet_id + n);
   if (lat->wall_distance) t.q.assign(lat->wall_distance, lat->wall_distance + 18 * n);
   if (lat->wall_normal) t.normal.assign(lat->wall_normal, lat->wall_normal + 3 * n);
-  else t.normal.assign(3 * n, 0.0);
+  else t.normal.assign(3 * n, 0.0f);
   for (int64_t i = 0; i < n; i++) t.type_counts[t.collision_type(i)]++;
   if (lat->neighbours) t.nbr.assign(lat->neighbours, lat->neighbours + 19 * n);
-  else hb::build_neighbours(t);
   return t;
 }
 
@@ -477,10 +478,33 @@ int hb_geometry_open(const char* gmy_path, hb_geometry** out) {
   *out = nullptr;
   return guard(nullptr, [&] {
     auto g = std::make_unique<hb_geometry>();
+    const auto t0 = std::chrono::steady_clock::now();
     g->tables = hb::read_gmy(gmy_path);
+    g->timing.read_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     *out = g.release();
     return HB_OK;
   });
+}
+
+int hb_geometry_open_device(const char* gmy_path, int device, hb_geometry** out) {
+  if (!gmy_path || !out) return HB_ERR_ARG;
+  *out = nullptr;
+  return guard(nullptr, [&] {
+    auto g = std::make_unique<hb_geometry>();
+    g->tables = hb::read_gmy_device(gmy_path, device, &g->timing);
+    *out = g.release();
+    return HB_OK;
+  });
+}
+
+int hb_geometry_read_timing(const hb_geometry* g, double ms[5]) {
+  if (!g || !ms) return HB_ERR_ARG;
+  ms[0] = g->timing.read_ms;
+  ms[1] = g->timing.inflate_ms;
+  ms[2] = g->timing.h2d_ms;
+  ms[3] = g->timing.device_ms;
+  ms[4] = g->timing.d2h_ms;
+  return HB_OK;
 }
 
 int hb_geometry_site_count(const hb_geometry* g, int64_t* n, int64_t dims[3]) {
@@ -505,18 +529,24 @@ int hb_geometry_tables(const hb_geometry* g, int64_t* neighbours, uint32_t* wall
                        int32_t* site_type, int32_t* iolet_id, int64_t* coords, int64_t* type_counts,
                        double* wall_distance, double* wall_normal) {
   if (!g) return HB_ERR_ARG;
-  const hb::LatticeTables& t = g->tables;
-  const size_t n = (size_t)t.n;
-  if (neighbours) std::memcpy(neighbours, t.nbr.data(), n * 19 * sizeof(int64_t));
-  if (wall_mask) std::memcpy(wall_mask, t.wall.data(), n * sizeof(uint32_t));
-  if (iolet_mask) std::memcpy(iolet_mask, t.iolet.data(), n * sizeof(uint32_t));
-  if (site_type) std::memcpy(site_type, t.stype.data(), n * sizeof(int32_t));
-  if (iolet_id) std::memcpy(iolet_id, t.iolet_id.data(), n * sizeof(int32_t));
-  if (coords) std::memcpy(coords, t.coords.data(), n * 3 * sizeof(int64_t));
-  if (type_counts) std::memcpy(type_counts, t.type_counts, 6 * sizeof(int64_t));
-  if (wall_distance) std::memcpy(wall_distance, t.q.data(), n * 18 * sizeof(double));
-  if (wall_normal) std::memcpy(wall_normal, t.normal.data(), n * 3 * sizeof(double));
-  return HB_OK;
+  return guard(nullptr, [&] {
+    const hb::LatticeTables& t = g->tables;
+    const size_t n = (size_t)t.n;
+    if (neighbours) hb::neighbour_table(t, neighbours);
+    if (wall_mask) std::memcpy(wall_mask, t.wall.data(), n * sizeof(uint32_t));
+    if (iolet_mask) std::memcpy(iolet_mask, t.iolet.data(), n * sizeof(uint32_t));
+    if (site_type) std::memcpy(site_type, t.stype.data(), n * sizeof(int32_t));
+    if (iolet_id) std::memcpy(iolet_id, t.iolet_id.data(), n * sizeof(int32_t));
+    if (coords) std::memcpy(coords, t.coords.data(), n * 3 * sizeof(int64_t));
+    if (type_counts) std::memcpy(type_counts, t.type_counts, 6 * sizeof(int64_t));
+    if (wall_distance) {
+      if (t.q.empty()) return HB_ERR_ARG;
+      for (size_t k = 0; k < 18 * n; k++) wall_distance[k] = (double)t.q[k];
+    }
+    if (wall_normal)
+      for (size_t k = 0; k < 3 * n; k++) wall_normal[k] = (double)t.normal[k];
+    return HB_OK;
+  });
 }
 
 int hb_geometry_layout(const hb_geometry* g, const hb_params* params, int wall, int64_t stats[4]) {

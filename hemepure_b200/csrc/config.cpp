@@ -585,30 +585,39 @@ LatticeTables read_gmy(const std::string& path) {
           t.iolet[c] = r.iolet;
           t.stype[c] = r.stype;
           t.iolet_id[c] = r.iolet_id;
-          for (int d = 0; d < 18; d++) t.q[18 * c + d] = (double)r.dist[d];
+          for (int d = 0; d < 18; d++) t.q[18 * c + d] = r.dist[d];
           if (r.has_normal) {
             // Vector3D<float>::GetNormalised, in float.
             float nx = r.normal[0], ny = r.normal[1], nz = r.normal[2];
             if (nx == 0.0f && ny == 0.0f && nz == 0.0f) {
-              t.normal[3 * c] = t.normal[3 * c + 1] = t.normal[3 * c + 2] = 0.0;
+              t.normal[3 * c] = t.normal[3 * c + 1] = t.normal[3 * c + 2] = 0.0f;
             } else {
               volatile float m2 = nx * nx + ny * ny + nz * nz;
               float m = std::sqrt((float)m2);
-              t.normal[3 * c] = (double)(nx / m);
-              t.normal[3 * c + 1] = (double)(ny / m);
-              t.normal[3 * c + 2] = (double)(nz / m);
+              t.normal[3 * c] = nx / m;
+              t.normal[3 * c + 1] = ny / m;
+              t.normal[3 * c + 2] = nz / m;
             }
           } else {
-            t.normal[3 * c] = t.normal[3 * c + 1] = t.normal[3 * c + 2] = (double)HUGE_VALF;
+            t.normal[3 * c] = t.normal[3 * c + 1] = t.normal[3 * c + 2] = HUGE_VALF;
           }
         }
       }
-  build_neighbours(t);
   return t;
 }
 
 void build_neighbours(LatticeTables& t) {
+  std::vector<int64_t> nbr((size_t)Q * t.n);
+  neighbour_table(t, nbr.data());
+  t.nbr = std::move(nbr);
+}
+
+void neighbour_table(const LatticeTables& t, int64_t* out) {
   const int64_t n = t.n;
+  if (!t.nbr.empty()) {
+    std::memcpy(out, t.nbr.data(), (size_t)Q * n * sizeof(int64_t));
+    return;
+  }
   const int64_t D0 = t.dims[0], D1 = t.dims[1], D2 = t.dims[2];
   std::vector<int32_t> grid(D0 * D1 * D2, -1);
   for (int64_t c = 0; c < n; c++) {
@@ -619,9 +628,8 @@ void build_neighbours(LatticeTables& t) {
     if (g >= 0) throw Error{HB_ERR_BAD_INDEX, "two sites share coordinates"};
     g = (int32_t)c;
   }
-  t.nbr.resize(Q * n);
   for (int64_t c = 0; c < n; c++) {
-    t.nbr[Q * c] = Q * c;
+    out[Q * c] = Q * c;
     for (int d = 1; d < Q; d++) {
       const int64_t px = t.coords[3 * c] + cx(d), py = t.coords[3 * c + 1] + cy(d), pz = t.coords[3 * c + 2] + cz(d);
       int64_t v = n * Q;  // the rubbish slot
@@ -629,7 +637,7 @@ void build_neighbours(LatticeTables& t) {
         const int32_t g = grid[(px * D1 + py) * D2 + pz];
         if (g >= 0) v = (int64_t)g * Q + d;
       }
-      t.nbr[Q * c + d] = v;
+      out[Q * c + d] = v;
     }
   }
 }

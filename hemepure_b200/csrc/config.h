@@ -50,9 +50,10 @@ struct LatticeTables {
   std::vector<uint32_t> iolet;      // [n]
   std::vector<int32_t> stype;       // [n] 0 fluid 1 inlet 2 outlet
   std::vector<int32_t> iolet_id;    // [n]
-  std::vector<double> q;            // [n*18]
-  std::vector<double> normal;       // [n*3]
-  std::vector<int64_t> nbr;         // [n*19]
+  std::vector<float> q;             // [n*18] cut distances as the .gmy stores them (float; -1 no wall link)
+  std::vector<float> normal;        // [n*3] wall normal, normalised in float (HUGE_VALF without one)
+  std::vector<int64_t> nbr;         // [n*19] neighbourIndices, or empty: derived from the coordinates
+                                    // when asked for (neighbour_table)
 
   int collision_type(int64_t i) const {
     const bool w = wall[i] != 0;
@@ -75,7 +76,17 @@ std::complex<double> bessel_j0(const std::complex<double>& z, double tol_sq = 1e
 
 // GeometryReader::LoadAndDecompose on one rank + LatticeData construction.
 LatticeTables read_gmy(const std::string& path);
-// neighbourIndices from coordinates (LatticeData::InitialiseNeighbourLookup).
+// neighbourIndices from coordinates (LatticeData::InitialiseNeighbourLookup), into
+// out[n*19]; t.nbr itself when the tables carry one.
+void neighbour_table(const LatticeTables& t, int64_t* out);
+// Fills t.nbr.
 void build_neighbours(LatticeTables& t);
+
+// The same tables with the site records decoded, binned and linked on the GPU
+// (gmy_device.cu); wall-clock milliseconds of its phases in `timing`.
+struct GmyTiming {
+  double read_ms = 0, inflate_ms = 0, h2d_ms = 0, device_ms = 0, d2h_ms = 0;
+};
+LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* timing = nullptr);
 
 }  // namespace hb

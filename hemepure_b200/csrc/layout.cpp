@@ -17,9 +17,12 @@
 #include "layout.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <numeric>
+#include <thread>
 
 namespace hb {
 
@@ -45,6 +48,40 @@ int closest_direction(const double n[3]) {
   return bi;
 }
 
+namespace {
+
+// Runs f(begin, end) over [0, n) split across up to 16 host threads (one when n
+// is small).  f must not throw; passes report errors through an atomic code.
+template <class F>
+void parallel_for(int64_t n, F f) {
+  const int64_t chunk_min = 1 << 16;
+  int T = (int)std::min<int64_t>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())),
+                                 std::max<int64_t>(1, n / chunk_min));
+  if (T <= 1) {
+    f((int64_t)0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int k = 1; k < T; k++) pool.emplace_back([&, k] { f(n * k / T, n * (k + 1) / T); });
+  f((int64_t)0, n / T);
+  for (auto& th : pool) th.join();
+}
+
+// First error of a parallel pass (0 = none): HB_ERR_* code and message.
+struct PassError {
+  std::atomic<int> code{0};
+  const char* msg = nullptr;
+  void set(int c, const char* m) {
+    int z = 0;
+    if (code.compare_exchange_strong(z, c)) msg = m;
+  }
+  void raise() const {
+    if (code.load()) throw Error{code.load(), msg};
+  }
+};
+
+}  // namespace
+
 Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
   Layout L;
   const int64_t n64 = t.n;
@@ -54,116 +91,198 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
   L.n = n;
   L.np = ((n64 + 63) / 64) * 64;
   const int64_t D[3] = {t.dims[0], t.dims[1], t.dims[2]};
+  PassError err;
 
   // Dense grid of reference indices.
   std::vector<int32_t> grid(D[0] * D[1] * D[2], -1);
   auto gidx = [&](int64_t x, int64_t y, int64_t z) { return (x * D[1] + y) * D[2] + z; };
-  for (int i = 0; i < n; i++) grid[gidx(t.coords[3 * i], t.coords[3 * i + 1], t.coords[3 * i + 2])] = i;
+  parallel_for(n, [&](int64_t b, int64_t e) {
+    for (int64_t i = b; i < e; i++) {
+      const int64_t* c = &t.coords[3 * i];
+      if (c[0] < 0 || c[1] < 0 || c[2] < 0 || c[0] >= D[0] || c[1] >= D[1] || c[2] >= D[2]) {
+        err.set(HB_ERR_BAD_INDEX, "site coordinates outside the lattice");
+        return;
+      }
+      int32_t expected = -1;
+      if (!__atomic_compare_exchange_n(&grid[gidx(c[0], c[1], c[2])], &expected, (int32_t)i, false, __ATOMIC_RELAXED,
+                                       __ATOMIC_RELAXED)) {
+        err.set(HB_ERR_BAD_INDEX, "two sites share coordinates");
+        return;
+      }
+    }
+  });
+  err.raise();
+  // neighbourIndices[x*19 + d]: the tables' own when they carry one, else from the grid
+  // (LatticeData::InitialiseNeighbourLookup).
+  auto neighbour = [&](int x, int d) -> int64_t {
+    if (!t.nbr.empty()) return t.nbr[(size_t)x * Q + d];
+    const int64_t px = t.coords[3 * x] + cx(d), py = t.coords[3 * x + 1] + cy(d), pz = t.coords[3 * x + 2] + cz(d);
+    if (px < 0 || py < 0 || pz < 0 || px >= D[0] || py >= D[1] || pz >= D[2]) return n64 * Q;
+    const int32_t g = grid[gidx(px, py, pz)];
+    return g >= 0 ? (int64_t)g * Q + d : n64 * Q;
+  };
 
   // Run axis: fewest sites whose predecessor along the axis is not fluid.
   int64_t best_runs = -1;
   for (int a = 0; a < 3; a++) {
-    int64_t runs = 0;
-    for (int i = 0; i < n; i++) {
-      int64_t c[3] = {t.coords[3 * i], t.coords[3 * i + 1], t.coords[3 * i + 2]};
-      c[a] -= 1;
-      if (c[a] < 0 || grid[gidx(c[0], c[1], c[2])] < 0) runs++;
-    }
-    if (best_runs < 0 || runs < best_runs) {
-      best_runs = runs;
+    std::atomic<int64_t> runs{0};
+    parallel_for(n, [&](int64_t b, int64_t e) {
+      int64_t r = 0;
+      for (int64_t i = b; i < e; i++) {
+        int64_t c[3] = {t.coords[3 * i], t.coords[3 * i + 1], t.coords[3 * i + 2]};
+        c[a] -= 1;
+        if (c[a] < 0 || grid[gidx(c[0], c[1], c[2])] < 0) r++;
+      }
+      runs += r;
+    });
+    if (best_runs < 0 || runs.load() < best_runs) {
+      best_runs = runs.load();
       L.axis = a;
     }
   }
   const int a0 = L.axis, a1 = (a0 + 1) % 3, a2 = (a0 + 2) % 3;
 
-  // Storage order.
-  std::vector<int64_t> key(n);
-  for (int i = 0; i < n; i++) {
-    const int64_t* c = &t.coords[3 * i];
-    key[i] = (c[a2] * D[a1] + c[a1]) * D[a0] + c[a0];
-  }
+  // Storage order: rows along a0, ordered by (c[a2], c[a1]): the grid read in
+  // that order.  A site starts a run when its predecessor along a0 is not fluid.
   L.st2ref.resize(n);
-  std::iota(L.st2ref.begin(), L.st2ref.end(), 0);
-  std::sort(L.st2ref.begin(), L.st2ref.end(), [&](int x, int y) { return key[x] < key[y]; });
   L.ref2st.resize(n);
-  for (int s = 0; s < n; s++) L.ref2st[L.st2ref[s]] = s;
-
-  // Runs.
   std::vector<int> run_of(n);
+  {
+    const int64_t R = D[a2] * D[a1];  // rows
+    std::vector<int64_t> row_count(R + 1, 0);
+    auto cell = [&](int64_t row, int64_t k) {
+      int64_t c[3];
+      c[a2] = row / D[a1];
+      c[a1] = row % D[a1];
+      c[a0] = k;
+      return grid[gidx(c[0], c[1], c[2])];
+    };
+    parallel_for(R, [&](int64_t b, int64_t e) {
+      for (int64_t row = b; row < e; row++) {
+        int64_t m = 0;
+        for (int64_t k = 0; k < D[a0]; k++) m += cell(row, k) >= 0;
+        row_count[row + 1] = m;
+      }
+    });
+    for (int64_t row = 0; row < R; row++) row_count[row + 1] += row_count[row];
+    parallel_for(R, [&](int64_t b, int64_t e) {
+      for (int64_t row = b; row < e; row++) {
+        int64_t sidx = row_count[row];
+        for (int64_t k = 0; k < D[a0]; k++) {
+          const int32_t x = cell(row, k);
+          if (x < 0) continue;
+          L.st2ref[sidx] = x;
+          L.ref2st[x] = (int)sidx;
+          run_of[sidx] = (k == 0 || cell(row, k - 1) < 0) ? 1 : 0;  // run start flag, numbered below
+          sidx++;
+        }
+      }
+    });
+  }
   int runs = 0;
+  std::vector<int> run_start;
   for (int s = 0; s < n; s++) {
-    if (s == 0 || key[L.st2ref[s]] != key[L.st2ref[s - 1]] + 1) runs++;
+    if (run_of[s]) {
+      runs++;
+      run_start.push_back(s);
+    }
     run_of[s] = runs - 1;
   }
+  run_start.push_back(n);
   L.runs = runs;
 
   // Slot writers from the push semantics.  src[s*19+i]: storage index of the
   // bulk source, -2 own boundary rule, -1 no writer yet.
-  std::vector<int> src((size_t)n * Q, -1);
-  std::vector<uint8_t> writers((size_t)n * Q, 0);
-  for (int x = 0; x < n; x++) {
-    const int ct = t.collision_type(x);
-    const int sx = L.ref2st[x];
-    for (int d = 0; d < Q; d++) {
-      const bool io = d > 0 && ct >= 2 && ((t.iolet[x] >> (d - 1)) & 1u);
-      const bool wl = d > 0 && (ct == 1 || ct >= 4) && ((t.wall[x] >> (d - 1)) & 1u);
-      if (io || wl) {
-        const size_t slot = (size_t)sx * Q + inv(d);
-        writers[slot]++;
-        src[slot] = -2;
-      } else {
-        const int64_t target = t.nbr[(size_t)x * Q + d];
-        if (target == n64 * Q) continue;  // the rubbish slot
-        if (target < 0 || target > n64 * Q || target % Q != d)
-          throw Error{HB_ERR_BAD_INDEX, "neighbour index out of range or in the wrong direction"};
-        const int y = (int)(target / Q);
-        const size_t slot = (size_t)L.ref2st[y] * Q + d;
-        writers[slot]++;
-        src[slot] = sx;
+  const size_t nslots = (size_t)n * Q;
+  std::unique_ptr<int[]> src(new int[nslots]);           // filled in parallel: the first touch
+  std::unique_ptr<uint8_t[]> writers(new uint8_t[nslots]);  // of these pages dominates otherwise
+  parallel_for((int64_t)nslots, [&](int64_t b, int64_t e) {
+    std::fill(src.get() + b, src.get() + e, -1);
+    std::fill(writers.get() + b, writers.get() + e, (uint8_t)0);
+  });
+  parallel_for(n, [&](int64_t b, int64_t e) {
+    for (int64_t xx = b; xx < e; xx++) {
+      const int x = (int)xx;
+      const int ct = t.collision_type(x);
+      const int sx = L.ref2st[x];
+      for (int d = 0; d < Q; d++) {
+        const bool io = d > 0 && ct >= 2 && ((t.iolet[x] >> (d - 1)) & 1u);
+        const bool wl = d > 0 && (ct == 1 || ct >= 4) && ((t.wall[x] >> (d - 1)) & 1u);
+        if (io || wl) {
+          const size_t slot = (size_t)sx * Q + inv(d);
+          __atomic_fetch_add(&writers[slot], (uint8_t)1, __ATOMIC_RELAXED);
+          src[slot] = -2;
+        } else {
+          const int64_t target = neighbour(x, d);
+          if (target == n64 * Q) continue;  // the rubbish slot
+          if (target < 0 || target > n64 * Q || target % Q != d) {
+            err.set(HB_ERR_BAD_INDEX, "neighbour index out of range or in the wrong direction");
+            return;
+          }
+          const int y = (int)(target / Q);
+          const size_t slot = (size_t)L.ref2st[y] * Q + d;
+          __atomic_fetch_add(&writers[slot], (uint8_t)1, __ATOMIC_RELAXED);
+          src[slot] = sx;
+        }
       }
     }
-  }
-  for (size_t k = 0; k < writers.size(); k++) {
-    if (writers[k] != 1)
-      throw Error{HB_ERR_UNSUPPORTED, writers[k] == 0 ? "a distribution slot is never written in a step (inconsistent cut links)"
-                                                      : "a distribution slot is written twice in a step (inconsistent cut links)"};
-  }
+  });
+  err.raise();
+  parallel_for((int64_t)nslots, [&](int64_t b, int64_t e) {
+    for (int64_t k = b; k < e; k++)
+      if (writers[k] != 1) {
+        err.set(HB_ERR_UNSUPPORTED, writers[k] == 0 ? "a distribution slot is never written in a step (inconsistent cut links)"
+                                                    : "a distribution slot is written twice in a step (inconsistent cut links)");
+        return;
+      }
+  });
+  err.raise();
 
   // Run offsets, per direction: from the first site of the run whose slot is a
   // bulk pull.  A site follows its run when every bulk slot matches them.
   L.run_off.assign((size_t)runs * 20, 0);
-  std::vector<uint32_t> run_set(runs, 0u);
   L.meta.assign(n, 0);
   std::vector<char> plain(n, 0), regular(n, 0);
-  for (int s = 0; s < n; s++) {
-    const int r = run_of[s];
-    int* off = &L.run_off[(size_t)r * 20];
-    for (int i = 1; i < Q; i++) {
-      const int v = src[(size_t)s * Q + i];
-      if (v >= 0 && !((run_set[r] >> i) & 1u)) {
-        off[i] = v - s;
-        run_set[r] |= 1u << i;
+  parallel_for(runs, [&](int64_t b, int64_t e) {
+    for (int64_t r = b; r < e; r++) {
+      int* off = &L.run_off[(size_t)r * 20];
+      uint32_t set = 0;
+      for (int s = run_start[r]; s < run_start[r + 1]; s++)
+        for (int i = 1; i < Q; i++) {
+          const int v = src[(size_t)s * Q + i];
+          if (v >= 0 && !((set >> i) & 1u)) {
+            off[i] = v - s;
+            set |= 1u << i;
+          }
+        }
+    }
+  });
+  parallel_for(n, [&](int64_t b, int64_t e) {
+    for (int64_t ss = b; ss < e; ss++) {
+      const int s = (int)ss;
+      const int* off = &L.run_off[(size_t)run_of[s] * 20];
+      bool ok = src[(size_t)s * Q] == s, all_bulk = true;
+      for (int i = 1; i < Q; i++) {
+        const int v = src[(size_t)s * Q + i];
+        if (v < 0) all_bulk = false;
+        else if (v - s != off[i]) ok = false;
       }
+      regular[s] = ok;
+      plain[s] = ok && all_bulk && t.collision_type(L.st2ref[s]) == 0;
     }
-  }
-  for (int s = 0; s < n; s++) {
-    const int r = run_of[s];
-    const int* off = &L.run_off[(size_t)r * 20];
-    bool ok = src[(size_t)s * Q] == s, all_bulk = true;
-    for (int i = 1; i < Q; i++) {
-      const int v = src[(size_t)s * Q + i];
-      if (v < 0) all_bulk = false;
-      else if (v - s != off[i]) ok = false;
-    }
-    regular[s] = ok;
-    plain[s] = ok && all_bulk && t.collision_type(L.st2ref[s]) == 0;
-  }
+  });
 
   // General sites, binned by collision type.
   std::vector<int> gl;
-  for (int s = 0; s < n; s++)
-    if (!plain[s]) gl.push_back(s);
-  std::stable_sort(gl.begin(), gl.end(), [&](int u, int v) { return t.collision_type(L.st2ref[u]) < t.collision_type(L.st2ref[v]); });
+  {
+    int64_t bin[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < n; s++)
+      if (!plain[s]) bin[t.collision_type(L.st2ref[s]) + 1]++;
+    for (int k = 1; k < 7; k++) bin[k] += bin[k - 1];
+    gl.resize(bin[6]);
+    for (int s = 0; s < n; s++)
+      if (!plain[s]) gl[bin[t.collision_type(L.st2ref[s])]++] = s;
+  }
   const int G = (int)gl.size();
   L.G = G;
   L.bulk_sites = n - G;

@@ -43,6 +43,7 @@ EXPORTS = [
     "hb_batch_run", "hb_batch_get_macro", "hb_batch_member_info", "hb_batch_set_tuning", "hb_batch_stats",
     "hb_batch_prepare_xml", "hb_batch_prep_sites", "hb_batch_add_prepared", "hb_batch_prep_free",
     "hb_write_xtr_selected", "hb_geometry_select", "hb_read_case_iolet_table", "hb_iolet_velocity",
+    "hb_geometry_open_device", "hb_geometry_read_timing",
 ]
 
 # Extraction geometry selectors (the <geometry type="..."> of a <propertyoutput>).
@@ -61,7 +62,8 @@ class Unstable(HemeLBError):
 
 
 class Options(C.Structure):
-    _fields_ = [("kernel", C.c_int), ("wall", C.c_int), ("precision", C.c_int), ("device", C.c_int)]
+    _fields_ = [("kernel", C.c_int), ("wall", C.c_int), ("precision", C.c_int), ("device", C.c_int),
+                ("geometry_reader", C.c_int)]
 
 
 class Iolet(C.Structure):
@@ -145,6 +147,8 @@ def library() -> C.CDLL:
     L.hb_device_bytes.argtypes = [P, P]
     L.hb_read_case.argtypes = [C.c_char_p, I, P, C.c_char_p, C.c_size_t]
     L.hb_geometry_open.argtypes = [C.c_char_p, C.POINTER(P)]
+    L.hb_geometry_open_device.argtypes = [C.c_char_p, I, C.POINTER(P)]
+    L.hb_geometry_read_timing.argtypes = [P, P]
     L.hb_geometry_site_count.argtypes = [P, P, P]
     L.hb_geometry_tables.argtypes = [P] + [P] * 9
     L.hb_geometry_layout.argtypes = [P, P, I, P]
@@ -180,13 +184,17 @@ def _p(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
 
 
-def options(kernel="LBGK", wall="SBB", precision="fp64", device=0) -> Options:
+GEOMETRY_READERS = {"host": 0, "device": 1}
+
+
+def options(kernel="LBGK", wall="SBB", precision="fp64", device=0, geometry_reader="device") -> Options:
     o = Options()
     library().hb_default_options(C.byref(o))
     o.kernel = KERNELS[kernel]
     o.wall = WALLS[wall]
     o.precision = PRECISIONS[precision]
     o.device = int(device)
+    o.geometry_reader = GEOMETRY_READERS[geometry_reader]
     return o
 
 
@@ -195,10 +203,10 @@ class LBM:
 
     def __init__(self, xml_path: Optional[str] = None, kernel: str = "LBGK", wall: str = "SBB",
                  precision: str = "fp64", device: int = 0, lattice: Optional[Dict[str, np.ndarray]] = None,
-                 params: Optional[Params] = None):
+                 params: Optional[Params] = None, geometry_reader: str = "device"):
         L = library()
         self._h = C.c_void_p()
-        self._opt = options(kernel, wall, precision, device)
+        self._opt = options(kernel, wall, precision, device, geometry_reader)
         if xml_path is not None:
             rc = L.hb_create_from_xml(os.fspath(xml_path).encode(), C.byref(self._opt), C.byref(self._h))
         else:
@@ -319,6 +327,12 @@ class LBM:
         self._check(library().hb_get_wk3(self._h, int(group), int(index), _p(a)))
         return a
 
+    def read_timing(self) -> Dict[str, float]:
+        """Wall-clock milliseconds of the open's phases."""
+        ms = np.zeros(5)
+        library().hb_geometry_read_timing(self._g, _p(ms))
+        return dict(zip(("read", "inflate", "h2d", "device", "d2h"), ms.tolist()))
+
     def tables(self) -> Dict[str, np.ndarray]:
         n = self.n
         out = {"neighbours": np.empty((n, 19), np.int64), "wall_mask": np.empty(n, np.uint32),
@@ -404,11 +418,16 @@ def iolet_velocity(iolet: Iolet, x, t: int) -> np.ndarray:
 
 
 class Geometry:
-    """Reference-order lattice tables read by the library's host code (no GPU needed)."""
+    """Reference-order lattice tables of a `.gmy`: read by the library's host code
+    (no GPU needed), or with `device` set decoded, binned and linked on that GPU
+    (the blocks inflated on host threads); the tables are the same bit for bit."""
 
-    def __init__(self, gmy_path: str):
+    def __init__(self, gmy_path: str, device: Optional[int] = None):
         self._g = C.c_void_p()
-        rc = library().hb_geometry_open(os.fspath(gmy_path).encode(), C.byref(self._g))
+        if device is None:
+            rc = library().hb_geometry_open(os.fspath(gmy_path).encode(), C.byref(self._g))
+        else:
+            rc = library().hb_geometry_open_device(os.fspath(gmy_path).encode(), int(device), C.byref(self._g))
         if rc != HB_OK:
             raise HemeLBError(rc, last_create_error())
         n = C.c_int64()
@@ -416,6 +435,12 @@ class Geometry:
         library().hb_geometry_site_count(self._g, C.byref(n), _p(dims))
         self.n = int(n.value)
         self.dims = dims
+
+    def read_timing(self) -> Dict[str, float]:
+        """Wall-clock milliseconds of the open's phases."""
+        ms = np.zeros(5)
+        library().hb_geometry_read_timing(self._g, _p(ms))
+        return dict(zip(("read", "inflate", "h2d", "device", "d2h"), ms.tolist()))
 
     def tables(self) -> Dict[str, np.ndarray]:
         n = self.n

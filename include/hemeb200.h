@@ -58,6 +58,10 @@ extern "C" {
                                     src/lb/iolets/InOutLetFileVelocity.cc */
 #define HB_IOLET_WOMERSLEY 6     /* Ladd velocity, Womersley profile, src/lb/iolets/InOutLetWomersleyVelocity.cc */
 
+/* ---- where the .gmy site records are decoded (same tables either way) */
+#define HB_GEOMETRY_HOST 0       /* one host thread (GeometryReader's steps) */
+#define HB_GEOMETRY_DEVICE 1     /* inflate on host threads, decode, order and link on the GPU */
+
 /* ---- storage precision of the distributions */
 #define HB_STORE_FP64 0          /* plain form: FP64 storage and arithmetic */
 #define HB_STORE_FP32 1          /* f - w_i rho0 stored in FP32, FP32 collision */
@@ -73,6 +77,7 @@ typedef struct hb_options {
   int wall;       /* HB_WALL_* (the reference's HEMELB_WALL_BOUNDARY) */
   int precision;  /* HB_STORE_* */
   int device;     /* CUDA device ordinal */
+  int geometry_reader; /* HB_GEOMETRY_*: where hb_create_from_xml decodes the .gmy */
 } hb_options;
 
 /* One inlet or outlet in lattice units (reference: iolets::InOutLet and subclasses). */
@@ -302,6 +307,14 @@ int hb_iolet_velocity(const hb_iolet* iolet, const double x[3], uint64_t t, doub
 typedef struct hb_geometry hb_geometry;
 /* GeometryReader + LatticeData on one rank: the reference-order tables. */
 int hb_geometry_open(const char* gmy_path, hb_geometry** out);
+/* The same tables (bit for bit) with the site records decoded, binned into the
+ * contiguous order and linked into the neighbour table on GPU `device`; the
+ * blocks are inflated on a pool of host threads. */
+int hb_geometry_open_device(const char* gmy_path, int device, hb_geometry** out);
+/* Wall-clock milliseconds of the last open's phases: file read and header,
+ * inflate, host-to-device copy, device decode/order/link, device-to-host copy
+ * (host reader: all of it in ms[0]). */
+int hb_geometry_read_timing(const hb_geometry* g, double ms[5]);
 int hb_geometry_site_count(const hb_geometry* g, int64_t* n, int64_t dims[3]);
 /* Same arrays as hb_get_tables plus wall distances [n*18] and normals [n*3]. */
 int hb_geometry_tables(const hb_geometry* g, int64_t* neighbours, uint32_t* wall_mask, uint32_t* iolet_mask,
