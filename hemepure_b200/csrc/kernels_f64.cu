@@ -33,8 +33,12 @@ constexpr int kGeneralBlocksPerSM = 8;
 // Kernels
 // ---------------------------------------------------------------------------
 
+// Three blocks of 256 per SM: TRT otherwise takes 92 registers and runs two
+// (measured 0.228 -> 0.200 ms per launch on the 4M pipe, no spills); LBGK fits
+// in 80 anyway.  The LES kernel and the output steps would spill under the
+// bound and keep the compiler's allocation.
 template <int K, bool GATHER, bool MACRO>
-__global__ void __launch_bounds__(256) k_bulk(const StepArgs a) {
+__global__ void __launch_bounds__(256, (K == kLES || MACRO) ? 1 : 3) k_bulk(const StepArgs a) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const int r = __ldg(a.meta + s);
