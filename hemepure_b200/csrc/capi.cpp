@@ -158,7 +158,7 @@ int hb_pre_send(hb_handle* h) { return h ? HB_OK : HB_ERR_ARG; }
 int hb_pre_receive(hb_handle* h, uint32_t flags) {
   if (!h) return HB_ERR_ARG;
   return guard(h, [&] {
-    h->solver->pre_receive((flags & HB_STEP_MACRO) != 0);
+    h->solver->pre_receive((flags & HB_STEP_MACRO) != 0, 3, (flags & HB_STEP_STRESS) != 0);
     return HB_OK;
   });
 }
@@ -225,6 +225,14 @@ int hb_get_macro(hb_handle* h, double* density, double* velocity, double* wss) {
   if (!h) return HB_ERR_ARG;
   return guard(h, [&] {
     h->solver->get_macro(density, velocity, wss);
+    return HB_OK;
+  });
+}
+
+int hb_get_stress(hb_handle* h, int field, double* out) {
+  if (!h || !out) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->get_stress(field, out);
     return HB_OK;
   });
 }

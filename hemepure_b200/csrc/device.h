@@ -80,6 +80,10 @@ struct StepArgs {
   double* u;              // [3][np]
   double* wss;
   int* status;            // bit 0 unstable, bit 1 iolet radius, bit 2 bad neighbour
+  // Output steps that need the stress caches: the non-equilibrium momentum flux
+  // tensor (xx, xy, xz, yy, yz, zz) and the relaxation time of each site, [7][np];
+  // null otherwise.
+  double* pi;
 };
 
 // One row of per-step iolet values: the density of iolet idx (inlets 0-15,
@@ -97,6 +101,10 @@ void launch_step_f64(const StepArgs& a, int kernel, int wall, bool gather, bool 
 void launch_gather_f64(const StepArgs& a, int wall, void* stream);
 // Gather the pre-collision f straight into AoS reference order.
 void launch_gather_aos_f64(const StepArgs& a, int wall, const int* st2ref, double* aos, void* stream);
+// Stress caches in lattice units from StepArgs::pi and rho of an output step
+// (BaseStreamer::UpdateMinsAndMaxes, src/lb/streamers/BaseStreamer.h:123-217):
+// field HB_STRESS_*, `out` [k][np] in storage order, k the field's length.
+void launch_stress_field(const StepArgs& a, int field, double* out, void* stream);
 void launch_wk3_begin(WK3Dev* wk3, int nwk3, const double* cpl_buf, double* dens_row, void* stream);
 void launch_equilibrium_f64(double* f, int64_t np, int n, const double feq[19], void* stream);
 void launch_equilibrium_aos_f64(double* f, int n, const double feq[19], void* stream);

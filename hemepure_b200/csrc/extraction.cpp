@@ -98,6 +98,30 @@ struct XdrIn {
   }
 };
 
+// Floats per site of each OutputField type (LocalPropertyOutput::GetFieldLength,
+// src/extraction/LocalPropertyOutput.cc:367-391); 0 for an unknown type.
+uint32_t field_len(const std::string& f) {
+  if (f == "pressure" || f == "vonmisesstress" || f == "shearstress" || f == "shearrate" || f == "wallextension" ||
+      f == "mpirank")
+    return 1;
+  if (f == "velocity" || f == "traction" || f == "tangentialprojectiontraction" || f == "normalprojectiontraction")
+    return 3;
+  if (f == "stresstensor") return 6;
+  if (f == "distributions") return (uint32_t)Q;
+  return 0;
+}
+
+// The stress cache an OutputField type reads, or -1.
+int stress_field(const std::string& f) {
+  if (f == "vonmisesstress") return HB_STRESS_VON_MISES;
+  if (f == "shearrate") return HB_STRESS_SHEAR_RATE;
+  if (f == "stresstensor") return HB_STRESS_TENSOR;
+  if (f == "traction") return HB_STRESS_TRACTION;
+  if (f == "tangentialprojectiontraction") return HB_STRESS_TANGENTIAL_TRACTION;
+  if (f == "normalprojectiontraction") return HB_STRESS_NORMAL_TRACTION;
+  return -1;
+}
+
 std::vector<std::string> split_fields(const std::string& s) {
   std::vector<std::string> out;
   std::stringstream ss(s);
@@ -106,15 +130,13 @@ std::vector<std::string> split_fields(const std::string& s) {
     size_t a = item.find_first_not_of(" \t"), b = item.find_last_not_of(" \t");
     if (a == std::string::npos) continue;
     item = item.substr(a, b - a + 1);
-    if (item != "velocity" && item != "pressure" && item != "shearstress" && item != "distributions")
-      throw Error{HB_ERR_ARG, "Unrecognised field type '" + item + "'"};
+    if (field_len(item) == 0) throw Error{HB_ERR_ARG, "Unrecognised field type '" + item + "'"};
     out.push_back(item);
   }
   if (out.empty()) throw Error{HB_ERR_ARG, "no output fields"};
   return out;
 }
 
-uint32_t field_len(const std::string& f) { return f == "velocity" ? 3u : (f == "distributions" ? 19u : 1u); }
 
 std::vector<unsigned char> read_file(const std::string& path) {
   std::ifstream in(path, std::ios::binary);
@@ -220,9 +242,17 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
   if (s.time_step() <= 1) throw Error{HB_ERR_ARG, "no completed time step to write"};
   const uint64_t label = s.time_step() - 1;
   bool need_macro = false, need_f = false;
+  std::vector<double> stress[6];
   for (auto& f : fields) {
     if (f == "distributions") need_f = true;
-    else need_macro = true;
+    else if (f == "pressure" || f == "velocity" || f == "shearstress") need_macro = true;
+    const int sf = stress_field(f);
+    if (sf >= 0 && stress[sf].empty()) {
+      if (!s.stress_valid())
+        throw Error{HB_ERR_ARG, "the last step did not fill the stress caches (pass HB_STEP_MACRO | HB_STEP_STRESS)"};
+      stress[sf].resize((size_t)n * field_len(f));
+      s.get_stress(sf, stress[sf].data());
+    }
   }
   std::vector<double> rho, u, wss, fd;
   if (need_macro) {
@@ -242,6 +272,12 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
   const double mass = 1000.0 * dx * dx * dx;
   const double lattice_pressure = mass / (dx * dt * dt);
   const double lattice_speed = dx / dt;
+  const double lattice_time = dt;
+  // REFERENCE_PRESSURE_mmHg (src/constants.h:23), kept in the expressions so that
+  // signed zeros and the non-finite normals of sites off the wall come out as the
+  // reference's conversions give them.
+  constexpr double kRefPressureMmHg = 0.0;
+  const std::vector<float>& normal = t.normal;
 
   XdrOut hdr;
   {
@@ -280,6 +316,39 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
         rec.f32((float)(u[3 * i + 2] * lattice_speed));
       } else if (f == "shearstress") {
         rec.f32((float)(wss[i] * lattice_pressure));
+      } else if (f == "vonmisesstress") {
+        // ConvertStressToPhysicalUnits (src/util/UnitConverter.h:61-64).
+        rec.f32((float)(stress[HB_STRESS_VON_MISES][i] * lattice_pressure));
+      } else if (f == "shearrate") {
+        // ConvertShearRateToPhysicalUnits (src/util/UnitConverter.cc:48-52).
+        rec.f32((float)(stress[HB_STRESS_SHEAR_RATE][i] / lattice_time));
+      } else if (f == "stresstensor") {
+        // ConvertFullStressTensorToPhysicalUnits (UnitConverter.h:73-78): the
+        // upper triangle row by row, the reference pressure off the diagonal.
+        const double* st = &stress[HB_STRESS_TENSOR][(size_t)i * 6];
+        for (int k = 0; k < 6; k++) {
+          double v = st[k] * lattice_pressure;
+          if (k == 0 || k == 3 || k == 5) v += -kRefPressureMmHg * kMmHgToPascal;
+          rec.f32((float)v);
+        }
+      } else if (f == "traction") {
+        // ConvertTractionToPhysicalUnits (UnitConverter.h:90-96) with the site's
+        // wall normal (non-finite off the wall, LatticeData.cc:242-244).
+        const double* tr = &stress[HB_STRESS_TRACTION][(size_t)i * 3];
+        const double scale = lattice_speed * lattice_speed * 1000.0;
+        for (int k = 0; k < 3; k++) {
+          const double nk = (double)normal[(size_t)3 * i + k];
+          rec.f32((float)(tr[k] * scale - nk * kRefPressureMmHg * kMmHgToPascal));
+        }
+      } else if (f == "tangentialprojectiontraction" || f == "normalprojectiontraction") {
+        const int sf = stress_field(f);
+        for (int k = 0; k < 3; k++) rec.f32((float)(stress[sf][(size_t)i * 3 + k] * lattice_pressure));
+      } else if (f == "wallextension") {
+        // Rigid walls: no delegate here sets a wall extension (only the elastic
+        // GZS delegate does, GuoZhengShiElasticWallDelegate.h:70), so it is 0.
+        rec.f32((float)(0.0 * dx));
+      } else if (f == "mpirank") {
+        rec.f32((float)0);  // one rank
       } else {
         for (int k = 0; k < Q; k++) rec.f32((float)fd[(size_t)i * Q + k]);
       }

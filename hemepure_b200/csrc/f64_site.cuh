@@ -115,6 +115,30 @@ __device__ __forceinline__ double wss_mag(double tau, const double* fpost, const
   return sqrt(sq - ns * ns);
 }
 
+// Non-equilibrium momentum flux tensor of an output step, stored for the stress
+// caches: the lower triangle in CalculatePiTensor's order and rounding
+// (src/lb/lattices/Lattice.h:1353-1383) as xx, xy, xz, yy, yz, zz, then tau.
+__device__ __forceinline__ void store_pi(const StepArgs& a, int s, double tau, const double* fpost, const double* f) {
+  double pi[3][3];
+#pragma unroll
+  for (int p = 0; p < 3; p++)
+#pragma unroll
+    for (int r = 0; r <= p; r++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int l = 0; l < Q; l++) acc += (fpost[l] - f[l]) * (double)cc(p, l) * (double)cc(r, l);
+      pi[p][r] = acc * -(tau - 0.5);
+    }
+  double* o = a.pi + s;
+  o[0] = pi[0][0];
+  o[a.np] = pi[1][0];
+  o[2 * a.np] = pi[2][0];
+  o[3 * a.np] = pi[1][1];
+  o[4 * a.np] = pi[2][1];
+  o[5 * a.np] = pi[2][2];
+  o[6 * a.np] = tau;
+}
+
 // InOutLetParabolicVelocity::GetVelocity (src/lb/iolets/InOutLetParabolicVelocity.cc:30-58).
 __device__ __forceinline__ bool parabolic(const IoletDev& I, const double x[3], uint64_t t, double v[3]) {
   const double dx = x[0] - I.pos[0], dy = x[1] - I.pos[1], dz = x[2] - I.pos[2];
@@ -298,6 +322,12 @@ __device__ __forceinline__ void bulk_site_f64(const StepArgs& a, int s, int r) {
     a.u[a.np + s] = my / rho;
     a.u[2 * a.np + s] = mz / rho;
     a.wss[s] = kNoValue;
+    if (a.pi) {
+      double fp[Q];
+#pragma unroll
+      for (int i = 0; i < Q; i++) fp[i] = collide_one<K>(a, f, fneq, om, i);
+      store_pi(a, s, tau, fp, f);
+    }
   }
 }
 
@@ -444,6 +474,7 @@ __device__ __forceinline__ void general_site_f64(const StepArgs& a, int g) {
     } else {
       a.wss[s] = kNoValue;
     }
+    if (a.pi) store_pi(a, s, tau, fp, f);
   }
 }
 

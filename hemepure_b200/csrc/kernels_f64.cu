@@ -20,6 +20,7 @@
 //                   stored in f*_d(x), which nothing else reads (d points into the wall).
 #include <cuda_runtime.h>
 
+#include "../../include/hemeb200.h"
 #include "device.h"
 #include "f64_site.cuh"
 #include "hb_common.h"
@@ -127,6 +128,110 @@ __global__ void k_wk3_begin(WK3Dev* wk3, const double* cpl_buf, double* dens_row
     W.flow_old = flow_old;
     W.count_prev = W.cpl_count;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Stress caches of an output step from the tensor the step stored
+// (BaseStreamer::UpdateMinsAndMaxes, src/lb/streamers/BaseStreamer.h:123-217;
+// Lattice::CalculateVonMisesStress, CalculateShearRate, CalculateStressTensor,
+// CalculateTractionOnAPoint and the two projections, src/lb/lattices/Lattice.h:983-1180).
+// Every expression keeps the reference's association order.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void load_pi(const StepArgs& a, int s, double pi[3][3], double& tau) {
+  const double* o = a.pi + s;
+  pi[0][0] = o[0];
+  pi[1][0] = o[a.np];
+  pi[2][0] = o[2 * a.np];
+  pi[1][1] = o[3 * a.np];
+  pi[2][1] = o[4 * a.np];
+  pi[2][2] = o[5 * a.np];
+  tau = o[6 * a.np];
+  pi[0][1] = pi[1][0];
+  pi[0][2] = pi[2][0];
+  pi[1][2] = pi[2][1];
+}
+
+// sigma = -Pi - (rho - 1) cs^2 I: Matrix3D's `pi * -1.0` then addDiagonal(-pressure).
+__device__ __forceinline__ void stress_tensor(const double pi[3][3], double rho, double st[3][3]) {
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) st[r][c] = -1.0 * pi[r][c];
+  const double pressure = (rho - 1) * kCs2;
+#pragma unroll
+  for (int r = 0; r < 3; r++) st[r][r] += -pressure;
+}
+
+// Site-wide caches for every site; the traction family is zero off the wall
+// (k_stress_walls then fills the wall sites).
+__global__ void __launch_bounds__(256) k_stress_sites(const StepArgs a, int field, double* out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const int64_t np = a.np;
+  if (field >= HB_STRESS_TRACTION) {
+    out[s] = 0.0;
+    out[np + s] = 0.0;
+    out[2 * np + s] = 0.0;
+    return;
+  }
+  double pi[3][3], tau;
+  load_pi(a, s, pi, tau);
+  if (field == HB_STRESS_VON_MISES) {
+    const double sxx_yy = pi[0][0] - pi[1][1];
+    const double syy_zz = pi[1][1] - pi[2][2];
+    const double szz_xx = pi[2][2] - pi[0][0];
+    const double sxy = pi[0][1], syz = pi[1][2], szx = pi[2][0];
+    const double t1 = sxx_yy * sxx_yy + syy_zz * syy_zz + szz_xx * szz_xx;
+    const double t2 = sxy * sxy + syz * syz + szx * szx;
+    out[s] = sqrt(0.5 * (t1 + 6.0 * t2));
+  } else if (field == HB_STRESS_SHEAR_RATE) {
+    double sr = 0.0;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) sr += pi[r][c] * pi[r][c];
+    sr = sqrt(sr) / (-2.0 * kCs2 * a.rho[s]);
+    sr /= (tau - 0.5);
+    out[s] = sr;
+  } else {
+    double st[3][3];
+    stress_tensor(pi, a.rho[s], st);
+    out[s] = st[0][0];
+    out[np + s] = st[0][1];
+    out[2 * np + s] = st[0][2];
+    out[3 * np + s] = st[1][1];
+    out[4 * np + s] = st[1][2];
+    out[5 * np + s] = st[2][2];
+  }
+}
+
+// Traction sigma.n at wall sites and its tangential and normal projections.
+__global__ void __launch_bounds__(128) k_stress_walls(const StepArgs a, int field, double* out) {
+  const GeneralDev& G = a.gen;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.G) return;
+  if (__ldg(G.wall + g) == 0u) return;
+  const int s = __ldg(G.site + g);
+  const double nor[3] = {(double)__ldg(G.nrm + g), (double)__ldg(G.nrm + G.G + g), (double)__ldg(G.nrm + 2 * G.G + g)};
+  double pi[3][3], tau, st[3][3], t[3];
+  load_pi(a, s, pi, tau);
+  stress_tensor(pi, a.rho[s], st);
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    t[r] = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) t[r] += st[r][c] * nor[c];
+  }
+  double v[3] = {t[0], t[1], t[2]};
+  if (field != HB_STRESS_TRACTION) {
+    const double m = t[0] * nor[0] + t[1] * nor[1] + t[2] * nor[2];
+#pragma unroll
+    for (int k = 0; k < 3; k++) v[k] = field == HB_STRESS_NORMAL_TRACTION ? nor[k] * m : t[k] - nor[k] * m;
+  }
+  out[s] = v[0];
+  out[a.np + s] = v[1];
+  out[2 * a.np + s] = v[2];
 }
 
 struct Row19 {
@@ -251,6 +356,13 @@ void launch_gather_f64(const StepArgs& a, int wall, void* stream) {
   if (wall == kBFL) k_gather<kBFL><<<(a.n + b - 1) / b, b, 0, st>>>(a);
   else if (wall == kGZS) k_gather<kGZS><<<(a.n + b - 1) / b, b, 0, st>>>(a);
   else k_gather<kSBB><<<(a.n + b - 1) / b, b, 0, st>>>(a);
+}
+
+void launch_stress_field(const StepArgs& a, int field, double* out, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (a.n <= 0) return;
+  k_stress_sites<<<(a.n + 255) / 256, 256, 0, st>>>(a, field, out);
+  if (field >= HB_STRESS_TRACTION && a.gen.G > 0) k_stress_walls<<<(a.gen.G + 127) / 128, 128, 0, st>>>(a, field, out);
 }
 
 void launch_gather_aos_f64(const StepArgs& a, int wall, const int* st2ref, double* aos, void* stream) {

@@ -118,6 +118,29 @@ __device__ __forceinline__ double wss_mag_f(float tau, const float* gp, const fl
   return (double)sqrtf(fmaxf(sq - ns * ns, 0.0f));
 }
 
+// Momentum flux tensor of an output step for the stress caches (FP32 sums of the
+// shifted values: gp - g equals fp - f), stored as FP64 like store_pi.
+__device__ __forceinline__ void store_pi_f(const StepArgs& a, int s, float tau, const float* gp, const float* g) {
+  float pi[3][3];
+#pragma unroll
+  for (int p = 0; p < 3; p++)
+#pragma unroll
+    for (int r = 0; r <= p; r++) {
+      float acc = 0.0f;
+#pragma unroll
+      for (int l = 0; l < Q; l++) acc += (gp[l] - g[l]) * (float)(cc(p, l) * cc(r, l));
+      pi[p][r] = acc * -(tau - 0.5f);
+    }
+  double* o = a.pi + s;
+  o[0] = (double)pi[0][0];
+  o[a.np] = (double)pi[1][0];
+  o[2 * a.np] = (double)pi[2][0];
+  o[3 * a.np] = (double)pi[1][1];
+  o[4 * a.np] = (double)pi[2][1];
+  o[5 * a.np] = (double)pi[2][2];
+  o[6 * a.np] = (double)tau;
+}
+
 __device__ __forceinline__ bool parabolic_f(const IoletDev& I, const double x[3], uint64_t t, float v[3]) {
   const double dx = x[0] - I.pos[0], dy = x[1] - I.pos[1], dz = x[2] - I.pos[2];
   const double z = dx * I.nrm[0] + dy * I.nrm[1] + dz * I.nrm[2];
@@ -282,6 +305,12 @@ __device__ __forceinline__ void bulk_collide_m(const StepArgs& a, const MixArgs&
     a.u[a.np + s] = (double)(my / rho);
     a.u[2 * a.np + s] = (double)(mz / rho);
     a.wss[s] = kNoValue;
+    if (a.pi) {
+      float gp[Q];
+#pragma unroll
+      for (int i = 0; i < Q; i++) gp[i] = collide_one_f<K>(a, g, fneq, om, i);
+      store_pi_f(a, s, tau, gp, g);
+    }
   }
 }
 
@@ -433,6 +462,7 @@ __device__ __forceinline__ void general_site_m(const StepArgs& a, const MixArgs&
     } else {
       a.wss[s] = kNoValue;
     }
+    if (a.pi) store_pi_f(a, s, tau, gp, g);
   }
 }
 

@@ -385,10 +385,16 @@ void Solver::request_comms() {
   phase_open_ = true;
 }
 
-void Solver::pre_receive(bool macro, int which) {
+void Solver::pre_receive(bool macro, int which, bool stress) {
   if (!phase_open_) request_comms();
   if (macro) ensure_macro();
-  const StepArgs a = args();
+  stress = stress && macro;
+  if (stress && !pi_.p) {
+    pi_.alloc((size_t)7 * L_.np * sizeof(double));
+    dev_bytes_ += (int64_t)pi_.bytes;
+  }
+  StepArgs a = args();
+  a.pi = stress ? pi_.as<double>() : nullptr;
   if (which == 3 && L_.G > 0) {
     // The boundary kernel (general sites) is latency-bound and the bulk kernel
     // bandwidth-bound: run them side by side, both after the Windkessel update.
@@ -403,6 +409,7 @@ void Solver::pre_receive(bool macro, int which) {
   }
   check(cudaGetLastError(), "step kernel launch");
   phase_macro_ = macro;
+  phase_stress_ = stress;
 }
 
 void Solver::launch(const StepArgs& a, bool macro, int which, cudaStream_t st) {
@@ -434,6 +441,8 @@ void Solver::end_iteration() {
   phase_open_ = false;
   macro_valid_ = phase_macro_;
   phase_macro_ = false;
+  stress_valid_ = phase_stress_;
+  phase_stress_ = false;
 }
 
 int Solver::read_status() {
@@ -461,7 +470,7 @@ int Solver::step(int64_t nsteps, uint32_t flags) {
       phase_open_ = true;
       launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
       const bool macro = (flags & HB_STEP_MACRO) && (done + j == nsteps - 1);
-      pre_receive(macro);
+      pre_receive(macro, 3, (flags & HB_STEP_STRESS) != 0);
       end_iteration();
       launches += per_step;
     }
@@ -623,6 +632,46 @@ void Solver::get_macro(double* rho, double* u, double* wss) {
       u[3 * x + 2] = uu[2 * np + s];
     }
     if (wss) wss[x] = w[s];
+  }
+}
+
+int Solver::stress_len(int field) {
+  switch (field) {
+    case HB_STRESS_VON_MISES:
+    case HB_STRESS_SHEAR_RATE:
+      return 1;
+    case HB_STRESS_TENSOR:
+      return 6;
+    case HB_STRESS_TRACTION:
+    case HB_STRESS_TANGENTIAL_TRACTION:
+    case HB_STRESS_NORMAL_TRACTION:
+      return 3;
+    default:
+      throw Error{HB_ERR_ARG, "unknown stress field " + std::to_string(field)};
+  }
+}
+
+void Solver::get_stress(int field, double* out) {
+  const int k = stress_len(field);
+  if (!stress_valid_ || !pi_.p)
+    throw Error{HB_ERR_ARG, "no step has filled the stress caches (pass HB_STEP_MACRO | HB_STEP_STRESS)"};
+  const int n = L_.n;
+  const int64_t np = L_.np;
+  if (!stress_out_.p) {
+    stress_out_.alloc((size_t)6 * np * sizeof(double));
+    dev_bytes_ += (int64_t)stress_out_.bytes;
+  }
+  StepArgs a = args();
+  a.pi = pi_.as<double>();
+  launch_stress_field(a, field, stress_out_.as<double>(), stream_);
+  check(cudaGetLastError(), "stress field launch");
+  std::vector<double> v((size_t)k * np);
+  check(cudaMemcpyAsync(v.data(), stress_out_.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+        "stress download");
+  check(cudaStreamSynchronize(stream_), "get_stress");
+  for (int s = 0; s < n; s++) {
+    const int64_t x = L_.st2ref[s];
+    for (int c = 0; c < k; c++) out[x * k + c] = v[(size_t)c * np + s];
   }
 }
 

@@ -33,7 +33,8 @@ class Solver {
 
   // lb::LBM phases.
   void request_comms();
-  void pre_receive(bool macro, int which = 3);
+  // `stress` (with `macro`) also stores the momentum flux tensor for the stress caches.
+  void pre_receive(bool macro, int which = 3, bool stress = false);
   void end_iteration();
   int step(int64_t n, uint32_t flags);
   // `n` steps with CUDA events around each launch: ms[0] plain bulk kernel,
@@ -45,6 +46,9 @@ class Solver {
   void get_fs(double* f);
   void set_fs(const double* f);
   void get_macro(double* rho, double* u, double* wss);
+  // Stress cache HB_STRESS_* of the last stress step, AoS in reference order.
+  void get_stress(int field, double* out);
+  static int stress_len(int field);
   void get_wk3(int group, int index, double st[4]);
 
   const LatticeTables& tables() const { return t_; }
@@ -62,6 +66,7 @@ class Solver {
   double dx() const { return dx_; }
   const double* origin() const { return origin_; }
   bool macro_valid() const { return macro_valid_; }
+  bool stress_valid() const { return stress_valid_; }
   // Pre-collision f of the last completed step (what the reference's GetFNew
   // returns after EndIteration), AoS in reference order.  False if no step has
   // run since the last set_fs / get_fs.
@@ -100,6 +105,7 @@ class Solver {
   DeviceBuffer g_wom_, wom_amp_;     // Womersley link factors (allocated only with such an iolet)
   DeviceBuffer vtau_, iolets_, dens_, cpl_buf_, wk3_, status_;
   DeviceBuffer rho_, u_, wss_;
+  DeviceBuffer pi_, stress_out_;  // allocated at the first stress step
   DeviceBuffer sum_scratch_, sum_out_;
   int dens_rows_ = 0;
   int row_ = 0;                   // row of the density table used by the current step
@@ -108,6 +114,8 @@ class Solver {
   bool macro_valid_ = false;
   bool phase_open_ = false;
   bool phase_macro_ = false;
+  bool stress_valid_ = false;
+  bool phase_stress_ = false;
   uint64_t t_step_ = 1;
   double omega_ = 0, omega_minus_ = 0;
   double last_ms_ = 0;

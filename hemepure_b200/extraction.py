@@ -16,8 +16,13 @@ from typing import List
 
 from . import lbm
 
-# Fields the library writes (OutputField types of the collide-and-stream path).
-WRITABLE_FIELDS = ("pressure", "velocity", "shearstress", "distributions")
+# OutputField types (src/extraction/OutputField.h:17-31, SimConfig::DoIOForPropertyField,
+# src/configuration/SimConfig.cc:566-632), all written by the library.
+WRITABLE_FIELDS = ("pressure", "velocity", "shearstress", "vonmisesstress", "shearrate", "stresstensor", "traction",
+                   "tangentialprojectiontraction", "normalprojectiontraction", "wallextension", "distributions",
+                   "mpirank")
+# Types read from the stress caches: the step before such a record runs with stress=True.
+STRESS_FIELDS = tuple(lbm.STRESS_FIELDS)
 
 
 @dataclass
@@ -91,17 +96,22 @@ def property_outputs(xml_path: str) -> List[PropertyOutput]:
         for f in po.findall("field"):
             kind = f.get("type")
             if kind not in WRITABLE_FIELDS:
-                raise ValueError(f"field type '{kind}' is not written by this library")
+                raise ValueError(f"Unrecognised field type '{kind}'")
             fields.append(kind)
         out.append(PropertyOutput(file=file, period=int(po.get("period")), start=int(po.get("start", 0)),
                                   stop=int(po.get("stop", 1000000000)), geometry=_geometry(geom), fields=fields))
     return out
 
 
+def needs_stress(outputs: List[PropertyOutput], label: int) -> bool:
+    """Whether a record labelled `label` due now reads a stress cache."""
+    return any(o.due(label) and any(f in STRESS_FIELDS for f in o.fields) for o in outputs)
+
+
 def write_due(sim: "lbm.LBM", outputs: List[PropertyOutput], directory: str) -> List[str]:
     """Append a record to every output due for the step just completed; returns
     the files written.  Outputs other than distributions need the step run with
-    the macroscopic caches filled."""
+    the macroscopic caches filled, and the stress types with the stress caches."""
     label = sim.time_step - 1
     written = []
     for o in outputs:

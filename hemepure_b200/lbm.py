@@ -29,13 +29,17 @@ WALLS = {"SBB": 0, "BFL": 1, "GZS": 2}
 PRECISIONS = {"fp64": 0, "fp32": 1, "fp16": 2}
 IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2, "wk2": 3, "file": 4, "file_velocity": 5, "womersley": 6}
 STEP_MACRO = 1
+STEP_STRESS = 2
+# Stress caches (HB_STRESS_*): name -> (index, values per site).
+STRESS_FIELDS = {"vonmisesstress": (0, 1), "shearrate": (1, 1), "stresstensor": (2, 6), "traction": (3, 3),
+                 "tangentialprojectiontraction": (4, 3), "normalprojectiontraction": (5, 3)}
 
 # Every entry point include/hemeb200.h declares.
 EXPORTS = [
     "hb_default_options", "hb_create_from_xml", "hb_create", "hb_destroy", "hb_last_error",
     "hb_request_comms", "hb_pre_send", "hb_pre_receive", "hb_post_receive", "hb_end_iteration",
     "hb_step", "hb_site_count", "hb_time_step", "hb_get_params", "hb_get_fs", "hb_set_fs",
-    "hb_get_macro", "hb_get_wk3", "hb_get_tables", "hb_write_xtr", "hb_read_checkpoint",
+    "hb_get_macro", "hb_get_stress", "hb_get_wk3", "hb_get_tables", "hb_write_xtr", "hb_read_checkpoint",
     "hb_last_step_timing", "hb_device_bytes", "hb_read_case", "hb_geometry_open", "hb_geometry_site_count",
     "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_close", "hb_profile_steps",
     "hb_set_time_step", "hb_moment_sums", "hb_moment_sums_noalloc",
@@ -135,6 +139,7 @@ def library() -> C.CDLL:
     L.hb_get_fs.argtypes = [P, P]
     L.hb_set_fs.argtypes = [P, P]
     L.hb_get_macro.argtypes = [P, P, P, P]
+    L.hb_get_stress.argtypes = [P, I, P]
     L.hb_get_wk3.argtypes = [P, I, I, P]
     L.hb_get_tables.argtypes = [P, P, P, P, P, P, P, P]
     L.hb_write_xtr.argtypes = [P, C.c_char_p, C.c_char_p, C.c_char_p]
@@ -185,6 +190,10 @@ def _p(a: np.ndarray):
 
 
 GEOMETRY_READERS = {"host": 0, "device": 1}
+
+
+def _flags(macro: bool, stress: bool) -> int:
+    return (STEP_MACRO if macro else 0) | (STEP_STRESS if (macro and stress) else 0)
 
 
 def options(kernel="LBGK", wall="SBB", precision="fp64", device=0, geometry_reader="device") -> Options:
@@ -267,8 +276,8 @@ class LBM:
     def PreSend(self) -> None:
         self._check(library().hb_pre_send(self._h))
 
-    def PreReceive(self, macro: bool = False) -> None:
-        self._check(library().hb_pre_receive(self._h, STEP_MACRO if macro else 0))
+    def PreReceive(self, macro: bool = False, stress: bool = False) -> None:
+        self._check(library().hb_pre_receive(self._h, _flags(macro, stress)))
 
     def PostReceive(self) -> None:
         self._check(library().hb_post_receive(self._h))
@@ -276,9 +285,10 @@ class LBM:
     def EndIteration(self) -> None:
         self._check(library().hb_end_iteration(self._h))
 
-    def step(self, n: int = 1, macro: bool = False) -> None:
-        """`n` full time steps (all phases); `macro` fills the caches on the last."""
-        self._check(library().hb_step(self._h, int(n), STEP_MACRO if macro else 0))
+    def step(self, n: int = 1, macro: bool = False, stress: bool = False) -> None:
+        """`n` full time steps (all phases); `macro` fills the caches on the last,
+        `stress` (with `macro`) the stress caches too."""
+        self._check(library().hb_step(self._h, int(n), _flags(macro, stress)))
 
     # -- state ---------------------------------------------------------------------------
     @property
@@ -315,6 +325,16 @@ class LBM:
         w = np.empty(self.n)
         self._check(library().hb_get_macro(self._h, _p(rho), _p(u), _p(w)))
         return rho, u, w
+
+    def GetStress(self, field: str) -> np.ndarray:
+        """Stress cache `field` of the last stress step in lattice units, [n, k] in
+        reference order: "vonmisesstress", "shearrate" (k = 1), "stresstensor" (xx, xy,
+        xz, yy, yz, zz), "traction", "tangentialprojectiontraction",
+        "normalprojectiontraction" (k = 3, zero off the wall)."""
+        idx, k = STRESS_FIELDS[field]
+        out = np.empty((self.n, k))
+        self._check(library().hb_get_stress(self._h, idx, _p(out)))
+        return out
 
     def moment_sums(self) -> np.ndarray:
         """(total density, total momentum x, y, z) of the current distributions, FP64."""

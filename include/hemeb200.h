@@ -69,6 +69,15 @@ extern "C" {
 
 /* ---- hb_step flags */
 #define HB_STEP_MACRO 1u         /* fill density, velocity and wall-shear-stress on the last step */
+#define HB_STEP_STRESS 2u        /* with HB_STEP_MACRO: also fill the stress caches (hb_get_stress) */
+
+/* ---- stress caches (MacroscopicPropertyCache, src/lb/MacroscopicPropertyCache.h) */
+#define HB_STRESS_VON_MISES 0            /* [n]   vonMisesStressCache */
+#define HB_STRESS_SHEAR_RATE 1           /* [n]   shearRateCache */
+#define HB_STRESS_TENSOR 2               /* [n*6] stressTensorCache: xx, xy, xz, yy, yz, zz */
+#define HB_STRESS_TRACTION 3             /* [n*3] tractionCache (zero off the wall) */
+#define HB_STRESS_TANGENTIAL_TRACTION 4  /* [n*3] tangentialProjectionTractionCache */
+#define HB_STRESS_NORMAL_TRACTION 5      /* [n*3] normalProjectionTractionCache */
 
 typedef struct hb_handle hb_handle;
 
@@ -183,6 +192,13 @@ int hb_set_fs(hb_handle* h, const double* f);
  * [n*3], wall-shear-stress magnitude [n] (NO_VALUE = DBL_MAX off the wall).
  * Any pointer may be NULL. */
 int hb_get_macro(hb_handle* h, double* density, double* velocity, double* wss);
+/* Stress cache `field` (HB_STRESS_*) of the last HB_STEP_MACRO | HB_STEP_STRESS step,
+ * in lattice units and reference order, as BaseStreamer::UpdateMinsAndMaxes fills
+ * it (src/lb/streamers/BaseStreamer.h:123-217; Lattice.h:983-1180): the von Mises
+ * stress and shear rate of the non-equilibrium momentum flux tensor, the full stress
+ * tensor -Pi - (rho - 1) cs^2 I, and at wall sites the traction sigma.n with its
+ * tangential and normal projections. */
+int hb_get_stress(hb_handle* h, int field, double* out);
 /* Total density and momentum (x, y, z) of the distributions entering the next
  * step, summed in FP64 in a fixed order: the per-step mass and flux balance
  * the reference's monitoring computes on the host (src/lb/IncompressibilityChecker.hpp). */
@@ -200,8 +216,11 @@ int hb_get_tables(const hb_handle* h, int64_t* neighbours, uint32_t* wall_mask, 
 /* ---- extraction and checkpoint (src/extraction/) ---------------------------- */
 
 /* Write one .xtr output step (LocalPropertyOutput::Write, float32 XDR) for the
- * whole lattice with the listed fields ("velocity", "pressure", "shearstress",
- * "distributions"; comma-separated).  Appends a record if the file exists with
+ * whole lattice with the listed fields (comma-separated OutputField types:
+ * "pressure", "velocity", "shearstress", "vonmisesstress", "shearrate",
+ * "stresstensor", "traction", "tangentialprojectiontraction",
+ * "normalprojectiontraction", "wallextension", "distributions", "mpirank";
+ * the stress types need the step run with HB_STEP_STRESS).  Appends a record if the file exists with
  * a matching header; `offset_path` (may be NULL) receives the .off file. */
 int hb_write_xtr(hb_handle* h, const char* path, const char* fields, const char* offset_path);
 /* Extraction geometry selectors (the <geometry type=...> of a <propertyoutput>,

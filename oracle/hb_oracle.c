@@ -519,6 +519,7 @@ struct orc_sim {
   double* rho;
   double* u;
   double* wss;
+  double* stress;           /* [n*17] stress caches of the last macro step (allocated at the first) */
   double* vtau;
   int nthreads;
   uint64_t t;               /* 1-based time step */
@@ -684,6 +685,7 @@ void orc_sim_free(orc_sim* s) {
   free(s->rho);
   free(s->u);
   free(s->wss);
+  free(s->stress);
   free(s->vtau);
   free(s->cpl_u);
   free(s->cpl_flag);
@@ -793,6 +795,15 @@ void orc_sim_get_macro(const orc_sim* s, double* rho, double* u, double* wss) {
   if (wss) memcpy(wss, s->wss, sizeof(double) * (size_t)n);
 }
 
+int orc_sim_get_stress(const orc_sim* s, int field, double* out) {
+  static const int first[6] = {0, 1, 2, 8, 11, 14}, len[6] = {1, 1, 6, 3, 3, 3};
+  if (field < 0 || field > 5 || !s->stress) return -1;
+  const int64_t n = s->lat->n;
+  for (int64_t i = 0; i < n; i++)
+    for (int k = 0; k < len[field]; k++) out[i * len[field] + k] = s->stress[17 * i + first[field] + k];
+  return 0;
+}
+
 void orc_sim_get_wk3(const orc_sim* s, int group, int index, double st[4]) {
   const iolet_t* io = &s->io[group][index];
   st[0] = io->density;
@@ -892,6 +903,67 @@ static double wss_mag(double tau, const double* fpost, const double* f, const do
     ns += sv[a] * nor[a];
   }
   return sqrt(sq - ns * ns);
+}
+
+/* Stress caches of one site (BaseStreamer::UpdateMinsAndMaxes,
+ * src/lb/streamers/BaseStreamer.h:123-217), each from CalculatePiTensor
+ * (src/lb/lattices/Lattice.h:1353-1383) in the reference's order:
+ * o[0] CalculateVonMisesStress (:983-1002), o[1] CalculateShearRate (:1159-1175),
+ * o[2..7] CalculateStressTensor (:1096-1112) as xx, xy, xz, yy, yz, zz,
+ * o[8..10] CalculateTractionOnAPoint (:1017-1028; Matrix3D::timesVector,
+ * src/util/Matrix3D.cc:45-55), o[11..13] CalculateTangentialProjectionTraction
+ * (:1045-1057), o[14..16] CalculateNormalProjectionTraction (:1069-1077); the
+ * traction family only at wall sites, zero elsewhere. */
+static void stress_caches(double tau, double rho, const double* fpost, const double* f, int wall, const double* nor,
+                          double* o) {
+  double pi[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b <= a; b++) {
+      pi[a][b] = 0.0;
+      for (int l = 0; l < Q; l++) pi[a][b] += (fpost[l] - f[l]) * (double)CV[a][l] * (double)CV[b][l];
+      pi[a][b] *= -(tau - 0.5);
+    }
+  for (int a = 0; a < 3; a++)
+    for (int b = a + 1; b < 3; b++) pi[a][b] = pi[b][a];
+
+  const double sxx_yy = pi[0][0] - pi[1][1], syy_zz = pi[1][1] - pi[2][2], szz_xx = pi[2][2] - pi[0][0];
+  const double sxy = pi[0][1], syz = pi[1][2], szx = pi[2][0];
+  const double temp1 = sxx_yy * sxx_yy + syy_zz * syy_zz + szz_xx * szz_xx;
+  const double temp2 = sxy * sxy + syz * syz + szx * szx;
+  o[0] = sqrt(0.5 * (temp1 + 6.0 * temp2));
+
+  double sr = 0.0;
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) sr += pi[r][c] * pi[r][c];
+  sr = sqrt(sr) / (-2.0 * CS2 * rho);
+  sr /= (tau - 0.5);
+  o[1] = sr;
+
+  double st[3][3];
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) st[r][c] = -1.0 * pi[r][c];
+  const double pressure = (rho - 1) * CS2;
+  for (int r = 0; r < 3; r++) st[r][r] += -pressure;
+  o[2] = st[0][0];
+  o[3] = st[0][1];
+  o[4] = st[0][2];
+  o[5] = st[1][1];
+  o[6] = st[1][2];
+  o[7] = st[2][2];
+
+  for (int k = 8; k < 17; k++) o[k] = 0.0;
+  if (!wall) return;
+  double t[3];
+  for (int r = 0; r < 3; r++) {
+    t[r] = 0.0;
+    for (int c = 0; c < 3; c++) t[r] += st[r][c] * nor[c];
+  }
+  const double m = t[0] * nor[0] + t[1] * nor[1] + t[2] * nor[2];
+  for (int k = 0; k < 3; k++) {
+    o[8 + k] = t[k];
+    o[11 + k] = t[k] - nor[k] * m;
+    o[14 + k] = nor[k] * m;
+  }
 }
 
 /* GuoZhengShiDelegate::StreamLink for wall link iPrime. Returns 0 or -1. */
@@ -1017,6 +1089,7 @@ static int site_update(orc_sim* s, int64_t i, int want_macro) {
     s->u[3 * i + 1] = h.uy;
     s->u[3 * i + 2] = h.uz;
     s->wss[i] = l->wall[i] ? wss_mag(h.tau, h.fpost, h.f, &l->normal[3 * i]) : NO_VALUE;
+    stress_caches(h.tau, h.rho, h.fpost, h.f, l->wall[i] != 0, &l->normal[3 * i], &s->stress[17 * i]);
   }
   (void)n;
   return rc;
@@ -1037,6 +1110,7 @@ static void site_post_step(orc_sim* s, int64_t i) {
 int orc_sim_run(orc_sim* s, int64_t steps, int want_macro) {
   const orc_lattice* l = s->lat;
   const int64_t n = l->n;
+  if (want_macro && !s->stress) s->stress = (double*)calloc((size_t)(17 * n + 1), sizeof(double));
 #ifdef _OPENMP
   omp_set_num_threads(s->nthreads);
 #endif

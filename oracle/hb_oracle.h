@@ -91,6 +91,10 @@ uint64_t orc_sim_time_step(const orc_sim* s);
 void orc_sim_get_f(const orc_sim* s, double* f);
 void orc_sim_set_f(orc_sim* s, const double* f);
 void orc_sim_get_macro(const orc_sim* s, double* rho, double* u, double* wss);
+/* Stress cache `field` of the last macro step (0 von Mises [n], 1 shear rate [n],
+ * 2 stress tensor [n*6], 3 traction, 4 tangential, 5 normal projection [n*3]);
+ * -1 before any macro step or for an unknown field. */
+int orc_sim_get_stress(const orc_sim* s, int field, double* out);
 /* WK3 state of iolet `index` of `group` (0 inlets, 1 outlets):
  * density, densityNew, flowRate, flowRateOld. */
 void orc_sim_get_wk3(const orc_sim* s, int group, int index, double st[4]);

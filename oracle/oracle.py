@@ -83,6 +83,7 @@ def lib():
         L.orc_sim_get_f.argtypes = [P, P]
         L.orc_sim_set_f.argtypes = [P, P]
         L.orc_sim_get_macro.argtypes = [P, P, P, P]
+        L.orc_sim_get_stress.argtypes = [P, C.c_int, P]
         L.orc_sim_get_wk3.argtypes = [P, C.c_int, C.c_int, P]
         L.orc_sim_get_vtau.argtypes = [P, P]
         L.orc_iolet_velocity.argtypes = [C.POINTER(_Iolet), P, C.c_uint64, P]
@@ -256,6 +257,17 @@ class Simulation:
         wss = np.zeros(self.n)
         lib().orc_sim_get_macro(self._h, _ptr(rho), _ptr(u), _ptr(wss))
         return rho, u, wss
+
+    # Stress caches: name -> (field index, values per site), as in the library.
+    STRESS = {"vonmisesstress": (0, 1), "shearrate": (1, 1), "stresstensor": (2, 6), "traction": (3, 3),
+              "tangentialprojectiontraction": (4, 3), "normalprojectiontraction": (5, 3)}
+
+    def stress(self, field: str) -> np.ndarray:
+        idx, k = self.STRESS[field]
+        out = np.zeros((self.n, k))
+        if lib().orc_sim_get_stress(self._h, idx, _ptr(out)) != 0:
+            raise RuntimeError("no macro step has filled the stress caches")
+        return out
 
     def wk3(self, group: int, index: int):
         a = np.zeros(4)

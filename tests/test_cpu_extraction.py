@@ -119,3 +119,25 @@ def test_property_outputs_are_read_from_the_case(tmp_path):
     assert p.type == lbm.SELECTORS["plane"] and list(p.point) == [1e-4, 2e-4, 3e-4] and p.radius == 5e-4
     assert list(outs[2].geometry.point2) == [0, 0, 1e-3]
     assert outs[1].due(10) and not outs[1].due(11) and outs[2].due(0) and outs[2].due(14)
+    assert not extraction.needs_stress(outs, 10)
+
+
+def test_every_output_field_type_is_accepted(tmp_path):
+    """All twelve OutputField types of SimConfig::DoIOForPropertyField are read;
+    an unknown type is an error, as in the reference."""
+    v = vessels.Pipe(4, 16)
+    gmy = tmp_path / "p.gmy"
+    vessels.voxelise(v, str(gmy))
+    xml = tmp_path / "p.xml"
+    props = [{"file": "all.xtr", "period": 4, "fields": list(extraction.WRITABLE_FIELDS)}]
+    vessels.write_case_xml(str(xml), "p.gmy", v, vessels.CaseUnits(tau=0.8), 100, [vessels.PressureBC(1.001)],
+                           [vessels.PressureBC(0.999)], properties=props)
+    (o,) = extraction.property_outputs(str(xml))
+    assert o.fields == list(extraction.WRITABLE_FIELDS) and len(o.fields) == 12
+    assert extraction.needs_stress([o], 8) and not extraction.needs_stress([o], 9)
+    bad = tmp_path / "bad.xml"
+    vessels.write_case_xml(str(bad), "p.gmy", v, vessels.CaseUnits(tau=0.8), 100, [vessels.PressureBC(1.001)],
+                           [vessels.PressureBC(0.999)], properties=[{"file": "x.xtr", "period": 1,
+                                                                      "fields": ["vorticity"]}])
+    with pytest.raises(ValueError):
+        extraction.property_outputs(str(bad))

@@ -148,3 +148,42 @@ def test_equilibrium_is_steady_without_driving(case_dir, tmp_path):
     rho, u, _ = sim.macro()
     assert np.max(np.abs(u)) < 1e-15
     assert np.max(np.abs(sim.f() - f0)) < 1e-15
+
+
+def test_oracle_stress_caches(case_dir):
+    """The oracle's stress caches (Lattice.h:983-1180 on CalculatePiTensor) hang
+    together: the tensor is -Pi - (rho - 1) cs^2 I, von Mises and the shear rate
+    follow from Pi, the traction is sigma.n at wall sites and zero elsewhere, and its
+    projections add up to it.  (The reference's LatticeTests/UnitConverterTests
+    cases for these functions call an older four-argument signature with the
+    opposite sign of the pressure term, so they are not restated here.)"""
+    xml, gmy, info, kernel, wall, _ = make_small_case(case_dir, "pipe_r8")
+    orc = O.Simulation(xml, kernel, wall)
+    assert orc.run(60, macro=True) == 0
+    rho, u, wss = orc.macro()
+    st = orc.stress("stresstensor")
+    walls = wss < 1e300
+    nrm = lbm.Geometry(gmy).tables()["wall_normal"]
+    p = (rho - 1) * (1.0 / 3.0)
+    pi = -st.copy()
+    pi[:, [0, 3, 5]] -= p[:, None]
+    full = pi[:, [0, 1, 2, 1, 3, 4, 2, 4, 5]].reshape(-1, 3, 3)
+    scale = np.max(np.abs(full))
+    assert scale > 0
+    vm = np.sqrt(0.5 * ((full[:, 0, 0] - full[:, 1, 1]) ** 2 + (full[:, 1, 1] - full[:, 2, 2]) ** 2
+                        + (full[:, 2, 2] - full[:, 0, 0]) ** 2
+                        + 6.0 * (full[:, 0, 1] ** 2 + full[:, 1, 2] ** 2 + full[:, 2, 0] ** 2)))
+    assert np.allclose(orc.stress("vonmisesstress")[:, 0], vm, rtol=1e-9, atol=1e-12 * scale)
+    tau = 0.8
+    sr = np.sqrt(np.sum(full ** 2, axis=(1, 2))) / (-2.0 / 3.0 * rho) / (tau - 0.5)
+    assert np.allclose(orc.stress("shearrate")[:, 0], sr, rtol=1e-9, atol=1e-12 * scale)
+    sig = st[:, [0, 1, 2, 1, 3, 4, 2, 4, 5]].reshape(-1, 3, 3)
+    tr = orc.stress("traction")
+    assert np.all(tr[~walls] == 0.0)
+    wn = walls & np.isfinite(nrm[:, 0])
+    assert np.any(wn)
+    assert np.allclose(tr[wn], np.einsum("nij,nj->ni", sig[wn], nrm[wn]), rtol=1e-12, atol=1e-18)
+    tan, nor = orc.stress("tangentialprojectiontraction"), orc.stress("normalprojectiontraction")
+    assert np.allclose(tan[wn] + nor[wn], tr[wn], rtol=1e-12, atol=1e-18)
+    # tangential to the wall up to the float normal's |n|^2 - 1 (~1e-7)
+    assert np.allclose(np.sum(tan[wn] * nrm[wn], axis=1), 0.0, atol=1e-6 * np.max(np.abs(tr[wn])))
