@@ -176,7 +176,7 @@ def serving_leg(n_requests: int, device: int, case_root: str):
     rep.update({"stream": f"{n_requests} seeded vessels (pipe / Y-bifurcation / 50-75% stenosis), r~U[6,32], "
                           f"L~U[10,40]r, LBGK/TRT tau~U[0.51,1], pressure or parabolic inlet Re<=300, "
                           f"1000-20000 steps", "storage": tuning.precision,
-                "tuning": {"sites_per_thread": tuning.sites_per_thread, "block": tuning.block,
+                "tuning": {"form": tuning.form, "sites_per_thread": tuning.sites_per_thread, "block": tuning.block,
                            "capacity_MLUPS": tuning.mlups, "probe_requests": len(probe),
                            "probe_sites": int(sum(r.sites for r in probe)), "table": tuning.table},
                 "arrival_rate_per_s": rate, "geometry_generation_s": gen_s,

@@ -96,6 +96,9 @@ Batch::Batch(int64_t site_capacity, int64_t general_capacity, int max_lattices, 
   check(cudaSetDevice(device_), "cudaSetDevice");
   cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_);
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
+  check(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaEventCreate(&ev0_), "cudaEventCreate");
   check(cudaEventCreate(&ev1_), "cudaEventCreate");
   const size_t elem = precision == HB_STORE_FP16 ? 2 : 4;
@@ -140,8 +143,9 @@ Batch::Batch(int64_t site_capacity, int64_t general_capacity, int max_lattices, 
 Batch::~Batch() {
   if (stream_) cudaStreamSynchronize(stream_);
   if (graph_) cudaGraphExecDestroy(graph_);
-  for (cudaEvent_t e : {ev0_, ev1_})
+  for (cudaEvent_t e : {ev0_, ev1_, fork_, join_})
     if (e) cudaEventDestroy(e);
+  if (side_) cudaStreamDestroy(side_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -150,6 +154,12 @@ void Batch::set_tuning(int spt, int bulk_block) {
     throw Error{HB_ERR_ARG, "sites per thread must be 1 or 2 and the block 128 or 256 threads"};
   spt_ = spt;
   bulk_block_ = bulk_block;
+  dirty_ = true;
+}
+
+void Batch::set_step_form(int form) {
+  if (form != HB_BATCH_STEP_PERSISTENT && form != HB_BATCH_STEP_SPLIT) throw Error{HB_ERR_ARG, "unknown step form"};
+  form_ = form;
   dirty_ = true;
 }
 
@@ -394,7 +404,8 @@ void Batch::capture(int k) {
   const int64_t sites_hw = sites_.high_water(), gens_hw = gens_.high_water();
   const int span = bulk_block_ * spt_;
   const int bulk_tiles = (int)((sites_hw + span - 1) / span);
-  const int gen_tiles = (int)((gens_hw + bulk_block_ - 1) / bulk_block_);
+  const int gen_block = form_ == HB_BATCH_STEP_SPLIT ? kBatchGenBlock : bulk_block_;
+  const int gen_tiles = (int)((gens_hw + gen_block - 1) / gen_block);
   const int grid = std::max(1, std::min(bulk_tiles + gen_tiles, sm_count_ * std::max(1, per_sm)));
   const int macro_grid = 2 * sm_count_;
   const int64_t iols_hw = iols_.high_water();
@@ -448,7 +459,18 @@ void Batch::capture(int k) {
     b.bulk_tiles = bulk_tiles;
     b.gen_tiles = gen_tiles;
     launch_batch_begin(lat_.p, cos_.p, dens_.as<double>(), macro_list_.as<int>(), macro_count_.as<int>(), n_lat, stream_);
-    launch_batch_step(b, precision_, spt_, bulk_block_, grid, stream_);
+    if (form_ == HB_BATCH_STEP_SPLIT) {
+      // boundary tiles on the side stream beside the bulk tiles (a fork and a
+      // join inside the captured graph)
+      check(cudaEventRecord(fork_, stream_), "fork");
+      check(cudaStreamWaitEvent(side_, fork_, 0), "fork");
+      launch_batch_gen(b, precision_, side_);
+      check(cudaEventRecord(join_, side_), "join");
+      launch_batch_bulk(b, precision_, spt_, bulk_block_, stream_);
+      check(cudaStreamWaitEvent(stream_, join_, 0), "join");
+    } else {
+      launch_batch_step(b, precision_, spt_, bulk_block_, grid, stream_);
+    }
     launch_batch_ghosts(b, precision_, ghost_grid, stream_);
     launch_batch_macro(b, precision_, macro_grid, stream_);
   }

@@ -83,6 +83,9 @@ class Batch {
   int members() const { return (int)members_.size(); }
   int64_t active_sites() const;
   void set_tuning(int spt, int bulk_block);
+  // HB_BATCH_STEP_PERSISTENT or HB_BATCH_STEP_SPLIT.
+  void set_step_form(int form);
+  int step_form() const { return form_; }
   int spt() const { return spt_; }
   int bulk_block() const { return bulk_block_; }
   double last_ms() const { return last_ms_; }
@@ -107,12 +110,15 @@ class Batch {
   std::map<int, std::unique_ptr<BatchMember>> members_;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaStream_t side_ = nullptr;               // boundary tiles of the split form
+  cudaEvent_t fork_ = nullptr, join_ = nullptr;
   DeviceBuffer f_[2], ghost_[2];
   DeviceBuffer meta_, run_off_;
   DeviceBuffer g_site_, g_run_, g_wall_, g_iolet_, g_src_, g_q_, g_nrm_, g_io_, g_cpl_, g_xyz_, g_lat_;
   DeviceBuffer lat_, cos_, iolets_, dens_, lat_status_, macro_list_, macro_count_, io_moments_, iol_list_, iol_link_, rho_, u_, wss_;
   int cur_ = 0;
   int spt_ = 2, bulk_block_ = 256;
+  int form_ = HB_BATCH_STEP_PERSISTENT;
   int sm_count_ = 148;
   cudaGraphExec_t graph_ = nullptr;
   int graph_k_ = 0;

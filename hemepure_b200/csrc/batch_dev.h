@@ -66,6 +66,11 @@ void launch_batch_macro(const BatchArgs& b, int precision, int grid, void* strea
 void launch_fill_ghost(float* ghost, int64_t pitch, int64_t base, int64_t n, const float vals[18], void* stream);
 // One step of all running lattices not in their last step (persistent kernel).
 void launch_batch_step(const BatchArgs& b, int precision, int spt, int block, int grid, void* stream);
+// Split form: bulk tiles (grid b.bulk_tiles of `block` threads) and boundary tiles
+// (grid b.gen_tiles of kBatchGenBlock records), launched on two streams.
+constexpr int kBatchGenBlock = 128;
+void launch_batch_bulk(const BatchArgs& b, int precision, int spt, int block, void* stream);
+void launch_batch_gen(const BatchArgs& b, int precision, void* stream);
 int batch_occupancy(int precision, int spt, int block, int* blocks_per_sm);
 void launch_fill_shift(void* out, int64_t np, int64_t base, int64_t n, const float vals[19], int precision, void* stream);
 

@@ -442,6 +442,14 @@ int hb_batch_set_tuning(hb_batch* b, int sites_per_thread, int block) {
   });
 }
 
+int hb_batch_set_step_form(hb_batch* b, int form) {
+  if (!b) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    b->batch->set_step_form(form);
+    return HB_OK;
+  });
+}
+
 int hb_batch_stats(const hb_batch* b, double* last_block_ms, int64_t* active_sites, int64_t* device_bytes) {
   if (!b) return HB_ERR_ARG;
   if (last_block_ms) *last_block_ms = b->batch->last_ms();

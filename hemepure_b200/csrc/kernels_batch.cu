@@ -205,6 +205,25 @@ __global__ void __launch_bounds__(256, SPT == 1 ? 4 : 3) k_batch_step(const Batc
   }
 }
 
+// The split form of the step: the same tiles as two ordinary (non-persistent)
+// kernels that the graph runs side by side, so each gets its own register
+// budget and the hardware balances the blocks.  Boundary tiles are 128 records
+// (54 registers, no spills).  The bulk kernel alone needs 56 registers; held to
+// 40 (six 256-thread blocks per SM, 8 bytes spilled) it ran the serving probe
+// (11 requests, 8.1M sites) at 28.1-28.5k MLUPS against 26.4-27.9k at 56 and
+// 22.9k for the persistent kernel.
+template <class S, int SPT>
+__global__ void __launch_bounds__(256, SPT == 1 ? 6 : 3) k_batch_bulk(const BatchArgs b) {
+  const MixArgs m{b.fin, b.fout, b.gin, b.gout};
+  batch_bulk_tile<S, SPT>(b, m, blockIdx.x);
+}
+
+template <class S>
+__global__ void __launch_bounds__(128) k_batch_gen(const BatchArgs b) {
+  const MixArgs m{b.fin, b.fout, b.gin, b.gout};
+  batch_general_tile<S>(b, m, blockIdx.x);
+}
+
 // Iolet ghosts of the boundary records stepped by k_batch_step: the Nash
 // zeroth-order pressure and Ladd velocity rules of general_site_m, from the
 // record's post-collision values (in fout) and its pre-collision density and
@@ -389,6 +408,25 @@ void launch_batch_step(const BatchArgs& b, int precision, int spt, int block, in
     if (spt == 2) k_batch_step<float, 2><<<grid, block, 0, st>>>(b);
     else k_batch_step<float, 1><<<grid, block, 0, st>>>(b);
   }
+}
+
+void launch_batch_bulk(const BatchArgs& b, int precision, int spt, int block, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (b.bulk_tiles <= 0) return;
+  if (precision == HB_STORE_FP16) {
+    if (spt == 2) k_batch_bulk<__half, 2><<<b.bulk_tiles, block, 0, st>>>(b);
+    else k_batch_bulk<__half, 1><<<b.bulk_tiles, block, 0, st>>>(b);
+  } else {
+    if (spt == 2) k_batch_bulk<float, 2><<<b.bulk_tiles, block, 0, st>>>(b);
+    else k_batch_bulk<float, 1><<<b.bulk_tiles, block, 0, st>>>(b);
+  }
+}
+
+void launch_batch_gen(const BatchArgs& b, int precision, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (b.gen_tiles <= 0) return;
+  if (precision == HB_STORE_FP16) k_batch_gen<__half><<<b.gen_tiles, kBatchGenBlock, 0, st>>>(b);
+  else k_batch_gen<float><<<b.gen_tiles, kBatchGenBlock, 0, st>>>(b);
 }
 
 int batch_occupancy(int precision, int spt, int block, int* blocks_per_sm) {

@@ -29,6 +29,7 @@ WALLS = {"SBB": 0, "BFL": 1, "GZS": 2}
 PRECISIONS = {"fp64": 0, "fp32": 1, "fp16": 2}
 IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2, "wk2": 3, "file": 4, "file_velocity": 5, "womersley": 6}
 STEP_MACRO = 1
+BATCH_FORMS = {"persistent": 0, "split": 1}
 STEP_STRESS = 2
 # Stress caches (HB_STRESS_*): name -> (index, values per site).
 STRESS_FIELDS = {"vonmisesstress": (0, 1), "shearrate": (1, 1), "stresstensor": (2, 6), "traction": (3, 3),
@@ -44,7 +45,8 @@ EXPORTS = [
     "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_close", "hb_profile_steps",
     "hb_set_time_step", "hb_moment_sums", "hb_moment_sums_noalloc",
     "hb_batch_bytes", "hb_batch_create", "hb_batch_destroy", "hb_batch_add_xml", "hb_batch_add", "hb_batch_remove",
-    "hb_batch_run", "hb_batch_get_macro", "hb_batch_member_info", "hb_batch_set_tuning", "hb_batch_stats",
+    "hb_batch_run", "hb_batch_get_macro", "hb_batch_member_info", "hb_batch_set_tuning", "hb_batch_set_step_form",
+    "hb_batch_stats",
     "hb_batch_prepare_xml", "hb_batch_prep_sites", "hb_batch_add_prepared", "hb_batch_prep_free",
     "hb_write_xtr_selected", "hb_geometry_select", "hb_read_case_iolet_table", "hb_iolet_velocity",
     "hb_geometry_open_device", "hb_geometry_read_timing",
@@ -172,6 +174,7 @@ def library() -> C.CDLL:
     L.hb_batch_get_macro.argtypes = [P, I, P, P, P]
     L.hb_batch_member_info.argtypes = [P, I, P, P, P]
     L.hb_batch_set_tuning.argtypes = [P, I, I]
+    L.hb_batch_set_step_form.argtypes = [P, I]
     L.hb_batch_stats.argtypes = [P, P, P, P]
     L.hb_batch_prepare_xml.argtypes = [C.c_char_p, I, I, U64, C.POINTER(P)]
     L.hb_batch_prep_sites.argtypes = [P, P]
@@ -593,8 +596,12 @@ class Batch:
         self._check(library().hb_batch_member_info(self._b, int(slot), C.byref(n), C.byref(t), C.byref(st)))
         return int(n.value), int(t.value), int(st.value)
 
-    def set_tuning(self, sites_per_thread: int, block: int) -> None:
+    def set_tuning(self, sites_per_thread: int, block: int, form: str = "persistent") -> None:
+        """Launch shape of the step: sites per thread, threads per block, and the
+        form ("persistent": one kernel interleaving bulk and boundary tiles;
+        "split": the same tiles as two kernels side by side)."""
         self._check(library().hb_batch_set_tuning(self._b, int(sites_per_thread), int(block)))
+        self._check(library().hb_batch_set_step_form(self._b, BATCH_FORMS[form]))
 
     def stats(self):
         ms, act, by = C.c_double(), C.c_int64(), C.c_int64()

@@ -140,12 +140,13 @@ class Tuning:
     precision: str
     mlups: float
     table: Dict[str, float] = field(default_factory=dict)
+    form: str = "persistent"
 
 
 def autotune(probe: Sequence[Request], tolerance: float = 1e-4, device: int = 0, block_steps: int = 100,
              site_capacity: Optional[int] = None) -> Tuning:
-    """Pick sites per thread, threads per block and storage precision, and
-    measure the batch's capacity in MLUPS.
+    """Pick the step form (persistent or split), sites per thread, threads per
+    block and storage precision, and measure the batch's capacity in MLUPS.
 
     Precision: FP16 storage is only eligible when the tolerance allows its error
     (about 1e-3 relative in velocity against FP64); otherwise FP32.  Each launch
@@ -161,16 +162,17 @@ def autotune(probe: Sequence[Request], tolerance: float = 1e-4, device: int = 0,
         b = lbm.Batch(cap, cap, max(8, len(probe)), precision=prec, device=device)
         for r in probe:
             b.add_xml(r.xml, r.kernel, r.wall, 10 ** 9)
-        for spt in (1, 2):
-            for block in (128, 256):
-                b.set_tuning(spt, block)
-                b.run(block_steps)          # capture + warm
-                b.run(block_steps)
-                ms, act, _ = b.stats()
-                mlups = act * block_steps / (ms * 1e-3) / 1e6
-                table[f"{prec}/spt{spt}/b{block}"] = mlups
-                if best is None or mlups > best.mlups:
-                    best = Tuning(spt, block, prec, mlups)
+        for form in ("persistent", "split"):
+            for spt in (1, 2):
+                for block in (128, 256):
+                    b.set_tuning(spt, block, form)
+                    b.run(block_steps)          # capture + warm
+                    b.run(block_steps)
+                    ms, act, _ = b.stats()
+                    mlups = act * block_steps / (ms * 1e-3) / 1e6
+                    table[f"{prec}/{form}/spt{spt}/b{block}"] = mlups
+                    if best is None or mlups > best.mlups:
+                        best = Tuning(spt, block, prec, mlups, form=form)
         b.close()
     best.table = table
     return best
@@ -215,7 +217,7 @@ class Server:
         self.site_capacity = lo
         self.batch = lbm.Batch(lo, int(lo * general_fraction), max_lattices, precision=precision, device=device)
         if tuning:
-            self.batch.set_tuning(tuning.sites_per_thread, tuning.block)
+            self.batch.set_tuning(tuning.sites_per_thread, tuning.block, tuning.form)
         self.block_steps = block_steps
         self.queue: deque = deque()
         self.prepared: Dict[int, Future] = {}
@@ -340,13 +342,14 @@ def _main(argv=None) -> None:
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"])
     ap.add_argument("--sites-per-thread", type=int, default=2)
     ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--form", default="persistent", choices=sorted(lbm.BATCH_FORMS))
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     reqs = generate_requests(a.requests, a.out, seed=a.seed)
     total = sum(r.sites for r in reqs)
     b = lbm.Batch(total + 64 * len(reqs) + 1024, total + 1024, max(8, len(reqs)), precision=a.precision)
-    b.set_tuning(a.sites_per_thread, a.block)
+    b.set_tuning(a.sites_per_thread, a.block, a.form)
     for r in reqs:
         b.add_xml(r.xml, r.kernel, r.wall, 10 ** 9)
     rows = []

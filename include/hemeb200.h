@@ -301,6 +301,13 @@ int hb_batch_get_macro(hb_batch* b, int slot, double* density, double* velocity,
 int hb_batch_member_info(hb_batch* b, int slot, int64_t* sites, uint64_t* time_step, int* status);
 /* Sites per thread (1, 2) and threads per block (128, 256) of the bulk kernel. */
 int hb_batch_set_tuning(hb_batch* b, int sites_per_thread, int block);
+/* Form of the step kernel: one persistent kernel interleaving bulk and boundary
+ * tiles (HB_BATCH_STEP_PERSISTENT, the default), or the same tiles as two ordinary
+ * kernels run side by side (HB_BATCH_STEP_SPLIT).  A tuning choice; results are
+ * identical. */
+#define HB_BATCH_STEP_PERSISTENT 0
+#define HB_BATCH_STEP_SPLIT 1
+int hb_batch_set_step_form(hb_batch* b, int form);
 /* Device time of the last block in ms, active sites, device bytes held. */
 int hb_batch_stats(const hb_batch* b, double* last_block_ms, int64_t* active_sites, int64_t* device_bytes);
 

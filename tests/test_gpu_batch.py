@@ -35,8 +35,10 @@ def mix(tmp_path_factory):
     return cases
 
 
-def run_alone(xml, kernel, wall, steps):
+def run_alone(xml, kernel, wall, steps, tuning=None):
     b = lbm.Batch(400_000, 200_000, 8)
+    if tuning:
+        b.set_tuning(*tuning)
     slot = b.add_xml(xml, kernel, wall, steps)
     done = []
     while not done:
@@ -116,3 +118,19 @@ def test_prepared_admission_matches_and_survives_refusal(mix):
         done = b.run(64)
     for a, m in zip(ref, b.macro(slot)):
         assert np.array_equal(a, m)
+
+
+@pytest.mark.parametrize("tuning", [(1, 256, "split"), (2, 128, "split"), (2, 256, "persistent"),
+                                    (1, 128, "persistent")])
+def test_every_launch_shape_gives_the_same_result(mix, tuning):
+    """The autotuner's choices (step form, sites per thread, block) change the
+    launch and, between kernel instantiations, where the compiler fuses FP32
+    multiply-adds: results agree to FP32 rounding (1e-5 of each field's largest
+    value), far inside the form's 1e-4 tolerance against FP64."""
+    for name, xml, kernel, wall, steps in mix:
+        ref = run_alone(xml, kernel, wall, steps)
+        got = run_alone(xml, kernel, wall, steps, tuning)
+        for a, m in zip(ref, got):
+            fin = a < 1e300
+            assert np.array_equal(fin, m < 1e300)
+            assert np.max(np.abs(a[fin] - m[fin])) <= 1e-5 * np.max(np.abs(a[fin])), (name, tuning)
