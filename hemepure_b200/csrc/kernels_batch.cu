@@ -207,8 +207,10 @@ __global__ void __launch_bounds__(256, SPT == 1 ? 4 : 3) k_batch_step(const Batc
 
 // The split form of the step: the same tiles as two ordinary (non-persistent)
 // kernels that the graph runs side by side, so each gets its own register
-// budget and the hardware balances the blocks.  Boundary tiles are 128 records
-// (54 registers, no spills).  The bulk kernel alone needs 56 registers; held to
+// budget and the hardware balances the blocks.  Boundary tiles are 128 records;
+// that kernel is latency-bound and held to 48 registers (ten blocks per SM, no
+// spills; 1.6-2% faster on the probe below than at its own 54).  The bulk kernel
+// alone needs 56 registers; held to
 // 40 (six 256-thread blocks per SM, 8 bytes spilled) it ran the serving probe
 // (11 requests, 8.1M sites) at 28.1-28.5k MLUPS against 26.4-27.9k at 56 and
 // 22.9k for the persistent kernel.
@@ -219,7 +221,7 @@ __global__ void __launch_bounds__(256, SPT == 1 ? 6 : 3) k_batch_bulk(const Batc
 }
 
 template <class S>
-__global__ void __launch_bounds__(128) k_batch_gen(const BatchArgs b) {
+__global__ void __launch_bounds__(128, 10) k_batch_gen(const BatchArgs b) {
   const MixArgs m{b.fin, b.fout, b.gin, b.gout};
   batch_general_tile<S>(b, m, blockIdx.x);
 }

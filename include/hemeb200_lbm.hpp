@@ -45,7 +45,12 @@ class LBM {
   // Per-step phases, in the order net::phased::StepManager calls them.
   void RequestComms() { check(hb_request_comms(h_)); }
   void PreSend() { check(hb_pre_send(h_)); }
-  void PreReceive(bool fill_property_cache = false) { check(hb_pre_receive(h_, fill_property_cache ? HB_STEP_MACRO : 0u)); }
+  // `fill_property_cache` fills density, velocity and wall shear stress; with
+  // `fill_stress_caches` also the von Mises, shear-rate, stress-tensor and traction caches.
+  void PreReceive(bool fill_property_cache = false, bool fill_stress_caches = false) {
+    check(hb_pre_receive(h_, (fill_property_cache ? HB_STEP_MACRO : 0u) |
+                                 (fill_property_cache && fill_stress_caches ? HB_STEP_STRESS : 0u)));
+  }
   void PostReceive() { check(hb_post_receive(h_)); }
   void EndIteration() { check(hb_end_iteration(h_)); }
 
@@ -78,6 +83,14 @@ class LBM {
     velocity.resize(3 * n);
     wss.resize(n);
     check(hb_get_macro(h_, density.data(), velocity.data(), wss.data()));
+  }
+  // One stress cache (HB_STRESS_*) of the last step run with the stress caches:
+  // 1, 6 (xx, xy, xz, yy, yz, zz) or 3 values per site, contiguous site order.
+  std::vector<double> GetStressCache(int field) const {
+    const size_t per = field == HB_STRESS_TENSOR ? 6 : (field >= HB_STRESS_TRACTION ? 3 : 1);
+    std::vector<double> out(per * (size_t)GetLocalFluidSiteCount());
+    check(hb_get_stress(h_, field, out.data()));
+    return out;
   }
   bool IsUnstable() const { return unstable_; }
   hb_handle* handle() const { return h_; }

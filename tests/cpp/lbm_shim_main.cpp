@@ -1,6 +1,7 @@
 // Drives the C++ class of include/hemeb200_lbm.hpp the way HemePure's
 // SimulationMaster drives lb::LBM: the five phases per step, the property
-// cache on the last step, then GetFOld and GetPropertyCache.  Writes the
+// and stress caches on the last step, then GetFOld, GetPropertyCache and the
+// stress tensor and traction caches.  Writes the
 // results as raw little-endian doubles for the test to compare.
 //
 //   lbm_shim_main <case.xml> <steps> <kernel 0|1|2> <wall 0|1|2> <out.bin>
@@ -29,7 +30,7 @@ int main(int argc, char** argv) {
     for (long t = 0; t < steps; t++) {
       lbm.RequestComms();
       lbm.PreSend();
-      lbm.PreReceive(t == steps - 1);
+      lbm.PreReceive(t == steps - 1, true);
       lbm.PostReceive();
       lbm.EndIteration();
     }
@@ -42,7 +43,9 @@ int main(int argc, char** argv) {
     std::ofstream out(argv[5], std::ios::binary);
     out.write(reinterpret_cast<const char*>(&n), sizeof n);
     out.write(reinterpret_cast<const char*>(&t), sizeof t);
-    const std::vector<double>* fields[] = {&f, &rho, &u, &wss};
+    const std::vector<double> tensor = lbm.GetStressCache(HB_STRESS_TENSOR);
+    const std::vector<double> traction = lbm.GetStressCache(HB_STRESS_TRACTION);
+    const std::vector<double>* fields[] = {&f, &rho, &u, &wss, &tensor, &traction};
     for (const std::vector<double>* v : fields)
       out.write(reinterpret_cast<const char*>(v->data()), (std::streamsize)(v->size() * sizeof(double)));
     return out ? 0 : 2;

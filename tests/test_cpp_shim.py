@@ -52,10 +52,12 @@ def test_shim_phases_match_the_oracle(shim, case_dir, tmp_path, key):
     raw = np.fromfile(out, dtype=np.uint8)
     n, t = np.frombuffer(raw[:16].tobytes(), dtype=np.int64)
     body = np.frombuffer(raw[16:].tobytes(), dtype=np.float64)
-    f, rho, u, wss = np.split(body, [19 * n, 20 * n, 23 * n])
+    f, rho, u, wss, tensor, traction = np.split(body, [19 * n, 20 * n, 23 * n, 24 * n, 30 * n])
     orc = O.Simulation(xml, kernel, wall)
     assert orc.run(steps, macro=True) == 0
     assert t == orc.time_step
     assert np.array_equal(f.reshape(n, 19), orc.f())
     rho_o, u_o, w_o = orc.macro()
     assert np.array_equal(rho, rho_o) and np.array_equal(u.reshape(n, 3), u_o) and np.array_equal(wss, w_o)
+    assert np.array_equal(tensor.reshape(n, 6), orc.stress("stresstensor"))
+    assert np.array_equal(traction.reshape(n, 3), orc.stress("traction"))
