@@ -101,7 +101,12 @@ Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& 
     omega_minus_ = -1.0 / tau_minus;
   }
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-  check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
+  // The latency-bound boundary kernel runs on the side stream at the highest
+  // priority, so its blocks are dispatched ahead of the bulk kernel's queued ones
+  // (4M-site pipe: FP32 step 29.3k -> 30.3k MLUPS; FP64 unchanged).
+  int prio_lo = 0, prio_hi = 0;
+  check(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi), "cudaDeviceGetStreamPriorityRange");
+  check(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, prio_hi), "cudaStreamCreate");
   check(cudaEventCreate(&ev0_), "cudaEventCreate");
   check(cudaEventCreate(&ev1_), "cudaEventCreate");
   check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
