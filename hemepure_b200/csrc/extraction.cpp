@@ -122,7 +122,10 @@ int stress_field(const std::string& f) {
   return -1;
 }
 
-std::vector<std::string> split_fields(const std::string& s) {
+// Comma-separated entries "type" or "type:name" (the <field type= name=> of a
+// <propertyoutput>; the name written in the header defaults to the type,
+// SimConfig::DoIOForPropertyField, src/configuration/SimConfig.cc:566-580).
+std::vector<std::string> split_fields(const std::string& s, std::vector<std::string>* names = nullptr) {
   std::vector<std::string> out;
   std::stringstream ss(s);
   std::string item;
@@ -130,8 +133,16 @@ std::vector<std::string> split_fields(const std::string& s) {
     size_t a = item.find_first_not_of(" \t"), b = item.find_last_not_of(" \t");
     if (a == std::string::npos) continue;
     item = item.substr(a, b - a + 1);
+    std::string name = item;
+    const size_t colon = item.find(':');
+    if (colon != std::string::npos) {
+      name = item.substr(colon + 1);
+      item = item.substr(0, colon);
+      if (name.empty()) throw Error{HB_ERR_ARG, "empty field name for type '" + item + "'"};
+    }
     if (field_len(item) == 0) throw Error{HB_ERR_ARG, "Unrecognised field type '" + item + "'"};
     out.push_back(item);
+    if (names) names->push_back(name);
   }
   if (out.empty()) throw Error{HB_ERR_ARG, "no output fields"};
   return out;
@@ -232,7 +243,8 @@ std::vector<uint8_t> select_sites(const LatticeTables& t, const hb_selector& sel
 
 void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv, const std::string& offset_path,
                const hb_selector* sel) {
-  const std::vector<std::string> fields = split_fields(fields_csv);
+  std::vector<std::string> names;
+  const std::vector<std::string> fields = split_fields(fields_csv, &names);
   const LatticeTables& t = s.tables();
   std::vector<uint8_t> take;
   if (sel) take = select_sites(t, *sel, s.dx(), s.origin());
@@ -282,8 +294,9 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
   XdrOut hdr;
   {
     XdrOut fh;
-    for (auto& f : fields) {
-      fh.str(f);
+    for (size_t k = 0; k < fields.size(); k++) {
+      const std::string& f = fields[k];
+      fh.str(names[k]);
       fh.u32(field_len(f));
       fh.f64(0.0);  // REFERENCE_PRESSURE_mmHg for pressure, 0 otherwise
     }

@@ -33,6 +33,13 @@ class PropertyOutput:
     stop: int
     geometry: lbm.Selector
     fields: List[str]
+    names: List[str] = None  # header name of each field (the type when the case gives none)
+
+    def field_specs(self) -> List[str]:
+        """The fields as the library's writer takes them: "type", or "type:name"
+        when the case names the field."""
+        names = self.names or self.fields
+        return [t if n == t else f"{t}:{n}" for t, n in zip(self.fields, names)]
 
     def due(self, time_step: int) -> bool:
         """LocalPropertyOutput::ShouldWrite for a record labelled `time_step`."""
@@ -92,14 +99,15 @@ def property_outputs(xml_path: str) -> List[PropertyOutput]:
         geom = po.find("geometry")
         if geom is None:
             raise ValueError("a <propertyoutput> needs a <geometry>")
-        fields = []
+        fields, names = [], []
         for f in po.findall("field"):
             kind = f.get("type")
             if kind not in WRITABLE_FIELDS:
                 raise ValueError(f"Unrecognised field type '{kind}'")
             fields.append(kind)
+            names.append(f.get("name", kind))
         out.append(PropertyOutput(file=file, period=int(po.get("period")), start=int(po.get("start", 0)),
-                                  stop=int(po.get("stop", 1000000000)), geometry=_geometry(geom), fields=fields))
+                                  stop=int(po.get("stop", 1000000000)), geometry=_geometry(geom), fields=fields, names=names))
     return out
 
 
@@ -117,6 +125,6 @@ def write_due(sim: "lbm.LBM", outputs: List[PropertyOutput], directory: str) -> 
     for o in outputs:
         if o.due(label):
             path = os.path.join(directory, o.file)
-            sim.WriteXtr(path, o.fields, geometry=o.geometry)
+            sim.WriteXtr(path, o.field_specs(), geometry=o.geometry)
             written.append(path)
     return written

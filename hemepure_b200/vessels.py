@@ -612,7 +612,9 @@ def write_case_xml(path: str, gmy_name: str, vessel: Vessel, units: CaseUnits, s
                     L.append(f'        <radius units="m" value="{float(geo["radius"])!r}"/>')
                 L.append('      </geometry>')
             for fld in po["fields"]:
-                L.append(f'      <field type="{fld}" />')
+                # "type" or "type:name"
+                kind, _, name = fld.partition(":")
+                L.append(f'      <field type="{kind}" name="{name}" />' if name else f'      <field type="{kind}" />')
             L.append('    </propertyoutput>')
         L.append('  </properties>')
     L.append('</hemelbsettings>')

@@ -219,7 +219,8 @@ int hb_get_tables(const hb_handle* h, int64_t* neighbours, uint32_t* wall_mask, 
  * whole lattice with the listed fields (comma-separated OutputField types:
  * "pressure", "velocity", "shearstress", "vonmisesstress", "shearrate",
  * "stresstensor", "traction", "tangentialprojectiontraction",
- * "normalprojectiontraction", "wallextension", "distributions", "mpirank";
+ * "normalprojectiontraction", "wallextension", "distributions", "mpirank", each
+ * optionally "type:name" to write the field under a name of its own;
  * the stress types need the step run with HB_STEP_STRESS).  Appends a record if the file exists with
  * a matching header; `offset_path` (may be NULL) receives the .off file. */
 int hb_write_xtr(hb_handle* h, const char* path, const char* fields, const char* offset_path);

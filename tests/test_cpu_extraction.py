@@ -135,6 +135,14 @@ def test_every_output_field_type_is_accepted(tmp_path):
     (o,) = extraction.property_outputs(str(xml))
     assert o.fields == list(extraction.WRITABLE_FIELDS) and len(o.fields) == 12
     assert extraction.needs_stress([o], 8) and not extraction.needs_stress([o], 9)
+    assert o.field_specs() == o.fields
+    named = tmp_path / "named.xml"
+    vessels.write_case_xml(str(named), "p.gmy", v, vessels.CaseUnits(tau=0.8), 100, [vessels.PressureBC(1.001)],
+                           [vessels.PressureBC(0.999)], properties=[{"file": "n.xtr", "period": 1,
+                                                                      "fields": ["velocity:v", "pressure"]}])
+    (n,) = extraction.property_outputs(str(named))
+    assert n.fields == ["velocity", "pressure"] and n.names == ["v", "pressure"]
+    assert n.field_specs() == ["velocity:v", "pressure"]
     bad = tmp_path / "bad.xml"
     vessels.write_case_xml(str(bad), "p.gmy", v, vessels.CaseUnits(tau=0.8), 100, [vessels.PressureBC(1.001)],
                            [vessels.PressureBC(0.999)], properties=[{"file": "x.xtr", "period": 1,

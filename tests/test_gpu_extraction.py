@@ -98,6 +98,22 @@ def test_xtr_fields_match_state(case_dir, tmp_path):
     assert o[4] == x["header_len"] and o[5] == x["header_len"] + x["rec_len"]
 
 
+def test_xtr_field_names(case_dir, tmp_path):
+    """A <field type= name=> is written under its name, with the type's values."""
+    xml, gmy, info, kernel, wall, _ = make_small_case(case_dir, "pipe_r8")
+    sim = lbm.LBM(xml, kernel=kernel, wall=wall)
+    sim.step(5, macro=True)
+    sim.WriteXtr(tmp_path / "a.xtr", ["velocity", "pressure"])
+    sim.WriteXtr(tmp_path / "b.xtr", ["velocity:inflow", "pressure:p"])
+    a, b = read_xtr(tmp_path / "a.xtr"), read_xtr(tmp_path / "b.xtr")
+    assert [(n, w) for n, w, _ in b["fields"]] == [("inflow", 3), ("p", 1)]
+    (_, _, va), = a["records"]
+    (_, _, vb), = b["records"]
+    assert np.array_equal(va["velocity"], vb["inflow"]) and np.array_equal(va["pressure"], vb["p"])
+    with pytest.raises(lbm.HemeLBError):
+        sim.WriteXtr(tmp_path / "c.xtr", ["velocity:"])
+
+
 def test_xtr_distributions_are_those_entering_the_step(case_dir, tmp_path):
     """A record labelled t carries the distributions that entered step t."""
     xml, gmy, info, kernel, wall, _ = make_small_case(case_dir, "pipe_r8")
