@@ -237,6 +237,15 @@ int hb_get_stress(hb_handle* h, int field, double* out) {
   });
 }
 
+int hb_set_iolet_densities(hb_handle* h, const double* inlet_density, int n_inlets, const double* outlet_density,
+                           int n_outlets) {
+  if (!h) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->set_iolet_densities(inlet_density, n_inlets, outlet_density, n_outlets);
+    return HB_OK;
+  });
+}
+
 int hb_moment_sums(hb_handle* h, double sums[4]) {
   if (!h || !sums) return HB_ERR_ARG;
   return guard(h, [&] {

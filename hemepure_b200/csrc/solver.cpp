@@ -361,6 +361,7 @@ void Solver::fill_density_rows(uint64_t t_first, int count) {
       if (idx % 16 < cnt) {
         const hb_iolet& c = idx < 16 ? p_.inlets[idx] : p_.outlets[idx - 16];
         if (c.kind == kFile) v = c.table[t0 < c.table_steps ? t0 : c.table_steps - 1];
+        if (dens_override_ && (c.kind == kCosine || c.kind == kFile)) v = dens_override_v_[idx];
         // Velocity iolets see BoundaryValues::GetTimeStep, the 1-based step as unsigned int.
         const uint64_t t1 = (uint64_t)(unsigned int)(t0 + 1);
         if (c.kind == kFileVelocity) va = c.table[t1 < c.table_steps ? t1 : c.table_steps - 1];
@@ -379,6 +380,18 @@ void Solver::fill_density_rows(uint64_t t_first, int count) {
   check(cudaMemcpyAsync(dens_.p, host_rows_.data(), (size_t)count * kRowStride * sizeof(double), cudaMemcpyHostToDevice,
                         stream_),
         "iolet row upload");
+}
+
+void Solver::set_iolet_densities(const double* inlets, int n_inlets, const double* outlets, int n_outlets) {
+  if (!inlets && !outlets) {
+    dens_override_ = false;
+    return;
+  }
+  if (!inlets || !outlets || n_inlets != p_.n_inlets || n_outlets != p_.n_outlets)
+    throw Error{HB_ERR_ARG, "iolet density override needs one value per inlet and per outlet of the case"};
+  for (int k = 0; k < n_inlets; k++) dens_override_v_[k] = inlets[k];
+  for (int k = 0; k < n_outlets; k++) dens_override_v_[16 + k] = outlets[k];
+  dens_override_ = true;
 }
 
 void Solver::request_comms() {

@@ -50,6 +50,9 @@ class Solver {
   void get_stress(int field, double* out);
   static int stress_len(int field);
   void get_wk3(int group, int index, double st[4]);
+  // Densities of the pressure iolets (cosine and file) supplied by the caller,
+  // replacing the ones computed from the case from the next step on; null clears.
+  void set_iolet_densities(const double* inlets, int n_inlets, const double* outlets, int n_outlets);
 
   const LatticeTables& tables() const { return t_; }
   const Layout& layout() const { return L_; }
@@ -110,6 +113,8 @@ class Solver {
   int dens_rows_ = 0;
   int row_ = 0;                   // row of the density table used by the current step
   std::vector<double> host_rows_;
+  bool dens_override_ = false;
+  double dens_override_v_[32] = {};  // inlets 0-15, outlets 16-31
   int nwk3_ = 0;
   bool macro_valid_ = false;
   bool phase_open_ = false;

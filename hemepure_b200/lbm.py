@@ -40,7 +40,7 @@ EXPORTS = [
     "hb_default_options", "hb_create_from_xml", "hb_create", "hb_destroy", "hb_last_error",
     "hb_request_comms", "hb_pre_send", "hb_pre_receive", "hb_post_receive", "hb_end_iteration",
     "hb_step", "hb_site_count", "hb_time_step", "hb_get_params", "hb_get_fs", "hb_set_fs",
-    "hb_get_macro", "hb_get_stress", "hb_get_wk3", "hb_get_tables", "hb_write_xtr", "hb_read_checkpoint",
+    "hb_get_macro", "hb_get_stress", "hb_set_iolet_densities", "hb_get_wk3", "hb_get_tables", "hb_write_xtr", "hb_read_checkpoint",
     "hb_last_step_timing", "hb_device_bytes", "hb_read_case", "hb_geometry_open", "hb_geometry_site_count",
     "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_close", "hb_profile_steps",
     "hb_set_time_step", "hb_moment_sums", "hb_moment_sums_noalloc",
@@ -142,6 +142,7 @@ def library() -> C.CDLL:
     L.hb_set_fs.argtypes = [P, P]
     L.hb_get_macro.argtypes = [P, P, P, P]
     L.hb_get_stress.argtypes = [P, I, P]
+    L.hb_set_iolet_densities.argtypes = [P, P, I, P, I]
     L.hb_get_wk3.argtypes = [P, I, I, P]
     L.hb_get_tables.argtypes = [P, P, P, P, P, P, P, P]
     L.hb_write_xtr.argtypes = [P, C.c_char_p, C.c_char_p, C.c_char_p]
@@ -338,6 +339,18 @@ class LBM:
         out = np.empty((self.n, k))
         self._check(library().hb_get_stress(self._h, idx, _p(out)))
         return out
+
+    def SetIoletDensities(self, inlets=None, outlets=None) -> None:
+        """Densities (lattice units) of every inlet and outlet used by the cosine and
+        file pressure iolets from the next step on, in place of the case's own
+        (BoundaryValues::GetBoundaryDensity supplied by the caller); no arguments
+        return to the case's values."""
+        if inlets is None and outlets is None:
+            self._check(library().hb_set_iolet_densities(self._h, None, 0, None, 0))
+            return
+        i = np.ascontiguousarray(inlets, dtype=np.float64)
+        o = np.ascontiguousarray(outlets, dtype=np.float64)
+        self._check(library().hb_set_iolet_densities(self._h, _p(i), len(i), _p(o), len(o)))
 
     def moment_sums(self) -> np.ndarray:
         """(total density, total momentum x, y, z) of the current distributions, FP64."""

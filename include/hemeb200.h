@@ -199,6 +199,15 @@ int hb_get_macro(hb_handle* h, double* density, double* velocity, double* wss);
  * tensor -Pi - (rho - 1) cs^2 I, and at wall sites the traction sigma.n with its
  * tangential and normal projections. */
 int hb_get_stress(hb_handle* h, int field, double* out);
+/* BoundaryValues::GetBoundaryDensity supplied by the caller (the per-step iolet
+ * values of src/lb/iolets/BoundaryValues.cc:211-214, for a HemePure host that keeps
+ * its own iolet objects or couples them to another model): lattice densities of
+ * every inlet and outlet, in the case's order, used by the cosine and file pressure
+ * iolets from the next step on in place of their own GetDensity (no warm-up blend);
+ * Windkessel densities stay on the device and velocity iolets ignore theirs.  The
+ * counts must be the case's; both pointers NULL returns to the case's values. */
+int hb_set_iolet_densities(hb_handle* h, const double* inlet_density, int n_inlets, const double* outlet_density,
+                           int n_outlets);
 /* Total density and momentum (x, y, z) of the distributions entering the next
  * step, summed in FP64 in a fixed order: the per-step mass and flux balance
  * the reference's monitoring computes on the host (src/lb/IncompressibilityChecker.hpp). */

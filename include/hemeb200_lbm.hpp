@@ -92,6 +92,12 @@ class LBM {
     check(hb_get_stress(h_, field, out.data()));
     return out;
   }
+  // BoundaryValues::GetBoundaryDensity from the caller's own iolets, per inlet and
+  // outlet, for the cosine and file pressure iolets from the next step on.
+  void SetIoletDensities(const std::vector<double>& inlets, const std::vector<double>& outlets) {
+    check(hb_set_iolet_densities(h_, inlets.data(), (int)inlets.size(), outlets.data(), (int)outlets.size()));
+  }
+  void ClearIoletDensities() { check(hb_set_iolet_densities(h_, nullptr, 0, nullptr, 0)); }
   bool IsUnstable() const { return unstable_; }
   hb_handle* handle() const { return h_; }
 
