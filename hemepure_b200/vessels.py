@@ -685,11 +685,20 @@ def make_case(name: str, out_dir: str, steps: Optional[int] = None, scale: float
         write_case_xml(xml, os.path.basename(gmy), v, u, steps or 8000,
                        [PressureBC(1.0, 1e-3, 4000.0)], outs, relaxation_parameter=3.0 / 16.0)
     elif name == "stenosis":
-        # Stenosed artery, LBGK+LES with outlet sponge, parabolic inlet.
+        # Stenosed artery, LBGK+LES with outlet sponge, pulsatile parabolic inlet:
+        # peak 0.05 (1 + 0.5 sin(2 pi t / 10^4)) lattice units from t = 0, as the
+        # reference's InOutLetFileVelocity (a parabolic profile whose peak speed
+        # is read from a file of time/speed pairs, one every 50 steps here).
         v = Stenosis(sc(48), sc(1200, 8), sc(24), max(4.0, 96 * scale))
         u = CaseUnits(tau=0.502)
-        write_case_xml(xml, os.path.basename(gmy), v, u, steps or 20000,
-                       [VelocityBC(0.05)], [PressureBC(1.0)],
+        n_steps = steps or 20000
+        table = os.path.join(out_dir, "stenosis_inflow.txt")
+        with open(table, "w") as fh:
+            for k in range(0, n_steps + 101, 50):
+                peak = 0.05 * (1.0 + 0.5 * math.sin(2.0 * math.pi * k / 10000.0))
+                fh.write(f"{k * u.dt!r} {u.speed_to_phys(peak)!r}\n")
+        write_case_xml(xml, os.path.basename(gmy), v, u, n_steps,
+                       [FileVelocityBC(os.path.basename(table))], [PressureBC(1.0)],
                        sponge={"viscosity_ratio": 10.0, "width": max(4.0, 60 * scale),
                                "lifetime": 2 * (steps or 20000)})
     else:
