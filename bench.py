@@ -302,9 +302,10 @@ def main():
     for _ in range(e2e_steps):
         sim.step(1)
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
-    e2e = {"value": world * n_sites * e2e_steps / e2e_s / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": 32 * 8,
+    e2e = {"value": world * n_sites * e2e_steps / e2e_s / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": 96 * 8,
            "d2h_bytes_per_step": 4, "steps": e2e_steps,
-           "note": "one hb_step(1) call per step: iolet densities up, stability word down, host sync"}
+           "note": "one hb_step(1) call per step: the step's iolet row (96 doubles, uploaded 1024 steps at a "
+                   "time), stability word down, host sync"}
 
     # The shifted low-precision forms on the same lattice (same step count).
     forms = {"fp64": {"MLUPS": value / world, "bytes_per_site": 304,

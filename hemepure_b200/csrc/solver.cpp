@@ -382,7 +382,21 @@ void Solver::fill_density_rows(uint64_t t_first, int count) {
         "iolet row upload");
 }
 
+// The rows depend on the step alone (the Windkessel kernel rewrites its own
+// entries of a row at that row's step), so a window of 1024 precomputed rows
+// serves consecutive hb_step calls of any length with one upload: a caller that
+// steps one step per call no longer uploads a row each step.
+int Solver::density_row(uint64_t t) {
+  if (!rows_valid_ || t < rows_first_ || t >= rows_first_ + (uint64_t)dens_rows_) {
+    fill_density_rows(t, dens_rows_);
+    rows_first_ = t;
+    rows_valid_ = true;
+  }
+  return (int)(t - rows_first_);
+}
+
 void Solver::set_iolet_densities(const double* inlets, int n_inlets, const double* outlets, int n_outlets) {
+  rows_valid_ = false;
   if (!inlets && !outlets) {
     dens_override_ = false;
     return;
@@ -395,10 +409,7 @@ void Solver::set_iolet_densities(const double* inlets, int n_inlets, const doubl
 }
 
 void Solver::request_comms() {
-  if (!phase_open_) {
-    fill_density_rows(t_step_, 1);
-    row_ = 0;
-  }
+  if (!phase_open_) row_ = density_row(t_step_);
   launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
   phase_open_ = true;
 }
@@ -479,20 +490,14 @@ int Solver::step(int64_t nsteps, uint32_t flags) {
   int64_t launches = 0;
   const int per_step = (nwk3_ ? 1 : 0) + (L_.n > 0 ? 1 : 0) + (L_.G > 0 ? 1 : 0);
   check(cudaEventRecord(ev0_, stream_), "event");
-  int64_t done = 0;
-  while (done < nsteps) {
-    const int chunk = (int)std::min<int64_t>(dens_rows_, nsteps - done);
-    fill_density_rows(t_step_, chunk);
-    for (int j = 0; j < chunk; j++) {
-      row_ = j;
-      phase_open_ = true;
-      launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
-      const bool macro = (flags & HB_STEP_MACRO) && (done + j == nsteps - 1);
-      pre_receive(macro, 3, (flags & HB_STEP_STRESS) != 0);
-      end_iteration();
-      launches += per_step;
-    }
-    done += chunk;
+  for (int64_t j = 0; j < nsteps; j++) {
+    row_ = density_row(t_step_);
+    phase_open_ = true;
+    launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
+    const bool macro = (flags & HB_STEP_MACRO) && (j == nsteps - 1);
+    pre_receive(macro, 3, (flags & HB_STEP_STRESS) != 0);
+    end_iteration();
+    launches += per_step;
   }
   check(cudaEventRecord(ev1_, stream_), "event");
   const int st = read_status();
@@ -513,12 +518,9 @@ int Solver::profile(int64_t nsteps, double ms[3]) {
   // Pass 0: the launches hb_step issues; pass 1: the bulk and boundary kernels
   // one after the other.
   for (int pass = 0; pass < 2; pass++) {
-    int64_t done = 0;
-    while (done < nsteps) {
-      const int chunk = (int)std::min<int64_t>(dens_rows_, nsteps - done);
-      fill_density_rows(t_step_, chunk);
-      for (int j = 0; j < chunk; j++) {
-        row_ = j;
+    for (int64_t j = 0; j < nsteps; j++) {
+      {
+        row_ = density_row(t_step_);
         phase_open_ = true;
         launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
         check(cudaEventRecord(e[0], stream_), "event");
@@ -543,7 +545,6 @@ int Solver::profile(int64_t nsteps, double ms[3]) {
           ms[2] += b;
         }
       }
-      done += chunk;
     }
   }
   for (auto& x : e) cudaEventDestroy(x);

@@ -81,6 +81,9 @@ class Solver {
   void materialise();
   void ensure_macro();
   void fill_density_rows(uint64_t t_first, int count);
+  // Index of step t's iolet row in the device table, refilling the table with
+  // the rows of steps t .. t + 1023 when t lies outside the resident window.
+  int density_row(uint64_t t);
   StepArgs args() const;
   void check(cudaError_t e, const char* what);
   bool mixed() const { return opt_.precision != HB_STORE_FP64; }
@@ -113,6 +116,8 @@ class Solver {
   int dens_rows_ = 0;
   int row_ = 0;                   // row of the density table used by the current step
   std::vector<double> host_rows_;
+  bool rows_valid_ = false;         // the device table holds the rows of steps rows_first_ ...
+  uint64_t rows_first_ = 0;
   bool dens_override_ = false;
   double dens_override_v_[32] = {};  // inlets 0-15, outlets 16-31
   int nwk3_ = 0;
