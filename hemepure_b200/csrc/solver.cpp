@@ -123,6 +123,7 @@ Solver::~Solver() {
   if (join_) cudaEventDestroy(join_);
   if (side_) cudaStreamDestroy(side_);
   if (stream_) cudaStreamDestroy(stream_);
+  if (status_host_) cudaFreeHost(status_host_);
 }
 
 void Solver::upload() {
@@ -259,6 +260,10 @@ void Solver::upload() {
   tot += (int64_t)dens_.bytes;
   host_rows_.assign((size_t)dens_rows_ * kRowStride, 1.0);
   status_.alloc(sizeof(int));
+  // The status word comes back after every hb_step call: a pinned host word makes
+  // that read a direct copy instead of a staged one.
+  check(cudaHostAlloc((void**)&status_host_, sizeof(int), cudaHostAllocDefault), "cudaHostAlloc");
+  *status_host_ = 0;
   check(cudaMemset(status_.p, 0, sizeof(int)), "cudaMemset");
   dev_bytes_ = tot;
 
@@ -475,9 +480,9 @@ void Solver::end_iteration() {
 }
 
 int Solver::read_status() {
-  int st = 0;
-  check(cudaMemcpyAsync(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "status read");
+  check(cudaMemcpyAsync(status_host_, status_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "status read");
   check(cudaStreamSynchronize(stream_), "step");
+  const int st = *status_host_;
   if (st) {
     status_sticky_ |= st;
     check(cudaMemsetAsync(status_.p, 0, sizeof(int), stream_), "status reset");

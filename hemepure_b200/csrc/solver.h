@@ -132,6 +132,7 @@ class Solver {
   int64_t last_launches_ = 0;
   int64_t dev_bytes_ = 0;
   int status_sticky_ = 0;
+  int* status_host_ = nullptr;    // pinned host copy of the status word
   bool prev_valid_ = false;
   bool prev_direct_ = false;
   double dt_ = 1.0, dx_ = 1.0;
