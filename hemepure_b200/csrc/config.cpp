@@ -191,7 +191,7 @@ CaseConfig read_case(const std::string& xml_path, int kernel) {
   }
   hb_params& p = c.params;
   std::memset(&p, 0, sizeof(p));
-  if (kernel == kTRT)
+  if (kernel == kTRT || kernel == kTRTSL)  // SimConfig.cc:165
     p.relaxation_parameter = parse_double(dim_value(sim.require("relaxation_parameter"), "lattice"), "relaxation_parameter");
   c.dx = parse_double(dim_value(sim.require("voxel_size"), "m"), "voxel_size");
   parse_vec(dim_value(sim.require("origin"), "m"), c.origin, "origin");
@@ -222,7 +222,7 @@ CaseConfig read_case(const std::string& xml_path, int kernel) {
   } else {
     c.checkpoint_file = ce->attr("file");
   }
-  if (kernel == kLES) {
+  if (is_sponge(kernel)) {  // SimConfig.cc:707
     const XmlElement& sp = ic.require("sponge_layer");
     p.viscosity_ratio = parse_double(dim_value(sp.require("viscosity_ratio"), "dimensionless"), "viscosity_ratio");
     p.sponge_width = u.to_lattice("m", parse_double(dim_value(sp.require("width"), "m"), "width"));

@@ -68,6 +68,7 @@ struct StepArgs {
   GeneralDev gen;
   // kernel parameters
   double tau, omega, omega_minus;
+  double lambda;          // TRT magic parameter (TRTSL: per-site omega_minus)
   const double* vtau;     // LES sponge tau per site (storage order) or null
   uint64_t t;             // 1-based time step of this step
   uint64_t lifetime;      // LES sponge lifetime

@@ -74,18 +74,50 @@ __device__ __forceinline__ double les_tau(const StepArgs& a, const double* fneq,
   return tau_les;
 }
 
-// Post-collision value of direction i for kernel K (LBGK.h:64-72, TRT.h:80-109).
+// Relaxation time of the LBGK and TRT sponge-layer kernels (CalculateTau,
+// src/lb/kernels/LBGKSpongeLayer.h:124-140, TRTSpongeLayer.h:157-172): the site's
+// sponge time for the first half of the lifetime, then a linear return to tau0.
+__device__ __forceinline__ double sponge_tau(const StepArgs& a, double vt) {
+  const double tau0 = a.tau;
+  if (a.t <= a.lifetime / 2) return vt;
+  if (a.t < a.lifetime) return (tau0 - vt) * 2.0 / (double)a.lifetime * (double)a.t + (2.0 * vt - tau0);
+  return tau0;
+}
+
+// Post-collision value of direction i for kernel K (LBGK.h:64-72, TRT.h:80-109,
+// and the sponge-layer kernels).  `omega_site` is the site's -1/tau for LBGK,
+// LES and LBGKSL, and its antisymmetric rate for TRTSL, whose symmetric rate stays
+// the global omega (TRTSpongeLayer.h:86-115).
 template <int K>
 __device__ __forceinline__ double collide_one(const StepArgs& a, const double* f, const double* fneq, double omega_site, int i) {
-  if (K == kTRT) {
-    if (i == 0) return f[0] + (0.5 * a.omega * (fneq[0] + fneq[0])) - (0.5 * a.omega_minus * (fneq[0] - fneq[0]));
+  if (K == kTRT || K == kTRTSL) {
+    const double omm = K == kTRT ? a.omega_minus : omega_site;
+    if (i == 0) return f[0] + (0.5 * a.omega * (fneq[0] + fneq[0])) - (0.5 * omm * (fneq[0] - fneq[0]));
     const int j = inv(i);
     const int lo = i < j ? i : j, hi = i < j ? j : i;
     const double sym = 0.5 * a.omega * (fneq[lo] + fneq[hi]);
-    const double asym = 0.5 * a.omega_minus * (fneq[lo] - fneq[hi]);
+    const double asym = 0.5 * omm * (fneq[lo] - fneq[hi]);
     return i == lo ? (f[i] + sym + asym) : (f[i] + sym - asym);
   }
   return f[i] + fneq[i] * omega_site;
+}
+
+// The site's relaxation time and the rate collide_one takes for kernel K.
+template <int K>
+__device__ __forceinline__ void site_rates(const StepArgs& a, const double* fneq, int s, double& tau, double& om) {
+  tau = a.tau;
+  om = a.omega;
+  if (K == kLES) {
+    tau = les_tau(a, fneq, __ldg(a.vtau + s));
+    om = -1.0 / tau;
+  } else if (K == kLBGKSL) {
+    tau = sponge_tau(a, __ldg(a.vtau + s));
+    om = -1.0 / tau;
+  } else if (K == kTRTSL) {
+    tau = sponge_tau(a, __ldg(a.vtau + s));
+    const double tau_minus = 0.5 + a.lambda / (tau - 0.5);
+    om = -1.0 / tau_minus;
+  }
 }
 
 // Wall-shear-stress magnitude (Lattice::CalculateWallShearStressMagnitude,
@@ -309,11 +341,8 @@ __device__ __forceinline__ void bulk_site_f64(const StepArgs& a, int s, int r) {
   double fneq[Q];
 #pragma unroll
   for (int i = 0; i < Q; i++) fneq[i] = f[i] - feq(i);
-  double om = a.omega, tau = a.tau;
-  if (K == kLES) {
-    tau = les_tau(a, fneq, __ldg(a.vtau + s));
-    om = -1.0 / tau;
-  }
+  double om, tau;
+  site_rates<K>(a, fneq, s, tau, om);
 #pragma unroll
   for (int i = 0; i < Q; i++) a.fout[(int64_t)i * a.np + s] = collide_one<K>(a, f, fneq, om, i);
   if (MACRO) {
@@ -351,11 +380,8 @@ __device__ __forceinline__ void general_site_f64(const StepArgs& a, int g) {
   double fneq[Q];
 #pragma unroll
   for (int i = 0; i < Q; i++) fneq[i] = f[i] - feq(i);
-  double om = a.omega, tau = a.tau;
-  if (K == kLES) {
-    tau = les_tau(a, fneq, __ldg(a.vtau + s));
-    om = -1.0 / tau;
-  }
+  double om, tau;
+  site_rates<K>(a, fneq, s, tau, om);
   double fp[Q];
 #pragma unroll
   for (int i = 0; i < Q; i++) fp[i] = collide_one<K>(a, f, fneq, om, i);

@@ -39,7 +39,9 @@ constexpr double kCs2 = 1.0 / 3.0;
 constexpr double kPi = 3.14159265358979323846264338327950288;
 constexpr double kNoValue = 1.7976931348623157e308;  // std::numeric_limits<double>::max()
 
-enum Kernel { kLBGK = 0, kTRT = 1, kLES = 2 };
+enum Kernel { kLBGK = 0, kTRT = 1, kLES = 2, kLBGKSL = 3, kTRTSL = 4 };
+// The kernels with a per-site sponge relaxation time.
+constexpr bool is_sponge(int k) { return k == kLES || k == kLBGKSL || k == kTRTSL; }
 enum Wall { kSBB = 0, kBFL = 1, kGZS = 2 };
 enum IoletKind { kCosine = 0, kWK3 = 1, kParabolic = 2, kWK2 = 3, kFile = 4, kFileVelocity = 5, kWomersley = 6 };
 // Velocity iolets take the Ladd streamer; the others the Nash zeroth-order pressure streamer.

@@ -36,10 +36,10 @@ constexpr int kGeneralBlocksPerSM = 8;
 
 // Three blocks of 256 per SM: TRT otherwise takes 92 registers and runs two
 // (measured 0.228 -> 0.200 ms per launch on the 4M pipe, no spills); LBGK fits
-// in 80 anyway.  The LES kernel and the output steps would spill under the
+// in 80 anyway.  The sponge-layer kernels and the output steps would spill under the
 // bound and keep the compiler's allocation.
 template <int K, bool GATHER, bool MACRO>
-__global__ void __launch_bounds__(256, (K == kLES || MACRO) ? 1 : 3) k_bulk(const StepArgs a) {
+__global__ void __launch_bounds__(256, (is_sponge(K) || MACRO) ? 1 : 3) k_bulk(const StepArgs a) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const int r = __ldg(a.meta + s);
@@ -50,10 +50,10 @@ __global__ void __launch_bounds__(256, (K == kLES || MACRO) ? 1 : 3) k_bulk(cons
 // The boundary kernel is latency-bound: with LBGK or TRT, bounce-back or BFL
 // walls and no outputs it is held to 64 registers so that 16 warps per SM hide
 // its dependent loads (it spills a little; LBGK/BFL measured 20% faster than at
-// 94 registers, and the whole step 5% faster).  The LES kernel, GZS walls and
+// 94 registers, and the whole step 5% faster).  The sponge-layer kernels, GZS walls and
 // output steps, which would spill far more, keep the compiler's allocation.
 template <int K, int WALL, bool GATHER, bool MACRO>
-__global__ void __launch_bounds__(128, (K != kLES && WALL != kGZS && !MACRO) ? kGeneralBlocksPerSM : 1)
+__global__ void __launch_bounds__(128, (!is_sponge(K) && WALL != kGZS && !MACRO) ? kGeneralBlocksPerSM : 1)
     k_general(const StepArgs a) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= a.gen.G) return;
@@ -346,7 +346,9 @@ void launch_step_f64(const StepArgs& a, int kernel, int wall, bool gather, bool 
   cudaStream_t st = (cudaStream_t)stream;
   if (kernel == kLBGK) launch1<kLBGK>(a, wall, gather, macro, which, bulk_block, general_block, st);
   else if (kernel == kTRT) launch1<kTRT>(a, wall, gather, macro, which, bulk_block, general_block, st);
-  else launch1<kLES>(a, wall, gather, macro, which, bulk_block, general_block, st);
+  else if (kernel == kLES) launch1<kLES>(a, wall, gather, macro, which, bulk_block, general_block, st);
+  else if (kernel == kLBGKSL) launch1<kLBGKSL>(a, wall, gather, macro, which, bulk_block, general_block, st);
+  else launch1<kTRTSL>(a, wall, gather, macro, which, bulk_block, general_block, st);
 }
 
 void launch_gather_f64(const StepArgs& a, int wall, void* stream) {

@@ -68,10 +68,12 @@ void upload_vec(DeviceBuffer& b, const std::vector<T>& v, int64_t& total) {
 
 Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& opt)
     : t_(std::move(tables)), p_(params), opt_(opt) {
-  if (opt_.kernel < 0 || opt_.kernel > 2 || opt_.wall < 0 || opt_.wall > 2) throw Error{HB_ERR_ARG, "unknown kernel or wall type"};
+  if (opt_.kernel < 0 || opt_.kernel > kTRTSL || opt_.wall < 0 || opt_.wall > 2) throw Error{HB_ERR_ARG, "unknown kernel or wall type"};
   if (opt_.precision < HB_STORE_FP64 || opt_.precision > HB_STORE_FP16) throw Error{HB_ERR_ARG, "unknown storage precision"};
-  if (opt_.kernel == kLES && opt_.wall == kGZS)
-    throw Error{HB_ERR_UNSUPPORTED, "GZS walls with the LES kernel: the virtual-node collision has no relaxation time"};
+  if (is_sponge(opt_.kernel) && opt_.wall == kGZS)
+    throw Error{HB_ERR_UNSUPPORTED, "GZS walls with a sponge-layer kernel: the virtual-node collision has no relaxation time"};
+  if ((opt_.kernel == kLBGKSL || opt_.kernel == kTRTSL) && opt_.precision != HB_STORE_FP64)
+    throw Error{HB_ERR_UNSUPPORTED, "the LBGKSL and TRTSL kernels run with FP64 storage"};
   if (!(p_.tau > 0.5)) throw Error{HB_ERR_ARG, "tau must exceed 1/2"};
   for (int k = 0; k < p_.n_inlets + p_.n_outlets; k++) {
     const hb_iolet& io = k < p_.n_inlets ? p_.inlets[k] : p_.outlets[k - p_.n_inlets];
@@ -191,7 +193,7 @@ void Solver::upload() {
 
   // LES sponge relaxation time per site (LBGKLESSpongeLayer::InitState,
   // src/lb/kernels/LBGKLESSpongeLayer.h:87-116), in storage order.
-  if (opt_.kernel == kLES) {
+  if (is_sponge(opt_.kernel)) {
     std::vector<double> vt(n);
     const double width = p_.sponge_width, widthsq = width * width;
     for (int s = 0; s < n; s++) {
@@ -321,6 +323,7 @@ StepArgs Solver::args() const {
   a.tau = p_.tau;
   a.omega = omega_;
   a.omega_minus = omega_minus_;
+  a.lambda = p_.relaxation_parameter;
   a.vtau = vtau_.as<double>();
   a.t = t_step_;
   a.lifetime = p_.sponge_lifetime;

@@ -24,7 +24,7 @@ HB_UNSTABLE = 1
 STATUS_NAMES = {1: "HB_UNSTABLE", -1: "HB_ERR_ARG", -2: "HB_ERR_IO", -3: "HB_ERR_FORMAT", -4: "HB_ERR_CUDA",
                 -5: "HB_ERR_OOM", -6: "HB_ERR_BAD_INDEX", -7: "HB_ERR_UNSUPPORTED", -8: "HB_ERR_IOLET_RADIUS",
                 -9: "HB_ERR_TIMEOUT"}
-KERNELS = {"LBGK": 0, "TRT": 1, "LBGKLESSL": 2}
+KERNELS = {"LBGK": 0, "TRT": 1, "LBGKLESSL": 2, "LBGKSL": 3, "TRTSL": 4}
 WALLS = {"SBB": 0, "BFL": 1, "GZS": 2}
 PRECISIONS = {"fp64": 0, "fp32": 1, "fp16": 2}
 IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2, "wk2": 3, "file": 4, "file_velocity": 5, "womersley": 6}

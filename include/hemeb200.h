@@ -44,6 +44,8 @@ extern "C" {
 #define HB_KERNEL_LBGK 0         /* src/lb/kernels/LBGK.h */
 #define HB_KERNEL_TRT 1          /* src/lb/kernels/TRT.h */
 #define HB_KERNEL_LBGKLESSL 2    /* src/lb/kernels/LBGKLESSpongeLayer.h */
+#define HB_KERNEL_LBGKSL 3       /* src/lb/kernels/LBGKSpongeLayer.h (FP64 storage) */
+#define HB_KERNEL_TRTSL 4        /* src/lb/kernels/TRTSpongeLayer.h (FP64 storage) */
 
 #define HB_WALL_SBB 0            /* src/lb/streamers/SimpleBounceBackDelegate.h */
 #define HB_WALL_BFL 1            /* src/lb/streamers/BouzidiFirdaousLallemandDelegate.h */

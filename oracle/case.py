@@ -226,7 +226,7 @@ def load_case(xml_path: str, kernel: str = "LBGK") -> CaseCfg:
         warmup = _val(wu_el, "lattice", int)
         steps += warmup
     relax = 0.0
-    if kernel in ("TRT",):
+    if kernel in ("TRT", "TRTSL"):  # SimConfig.cc:165
         relax = _val(sim.find("relaxation_parameter"), "lattice")
     dx = _val(sim.find("voxel_size"), "m")
     origin = _vec(sim.find("origin").get("value"))
@@ -244,7 +244,7 @@ def load_case(xml_path: str, kernel: str = "LBGK") -> CaseCfg:
     rho0 = u.pressure_to_lattice(p0) / CS2
     vr = sw = 0.0
     life = 0
-    if kernel == "LBGKLESSL":
+    if kernel in ("LBGKSL", "LBGKLESSL", "TRTSL"):  # SimConfig.cc:707
         sp = ic.find("sponge_layer")
         vr = _val(sp.find("viscosity_ratio"), "dimensionless")
         sw = u.to_lattice("m", _val(sp.find("width"), "m"))

@@ -697,9 +697,10 @@ void orc_sim_set_threads(orc_sim* s, int nthreads) { s->nthreads = nthreads > 0 
 int orc_sim_create(const orc_lattice* lat, const orc_params* p, orc_sim** out, char* err, int errlen) {
   init_tables();
   *out = NULL;
-  if (p->kernel == ORC_LBGKLES && p->wall == ORC_GZS) {
-    /* The GZS virtual-node collision reads a relaxation time that the LES kernel never sets. */
-    seterr(err, errlen, "GZS walls with the LES kernel are not supported");
+  if ((p->kernel == ORC_LBGKLES || p->kernel == ORC_LBGKSL || p->kernel == ORC_TRTSL) && p->wall == ORC_GZS) {
+    /* The GZS virtual-node collision reads a relaxation time that the sponge-layer
+     * kernels (LES or not) never set on the wall node's HydroVars. */
+    seterr(err, errlen, "GZS walls with a sponge-layer kernel are not supported");
     return -1;
   }
   orc_sim* s = (orc_sim*)calloc(1, sizeof(orc_sim));
@@ -757,8 +758,9 @@ int orc_sim_create(const orc_lattice* lat, const orc_params* p, orc_sim** out, c
   for (int g = 0; g < 2; g++)
     for (int k = 0; k < s->nio[g]; k++) s->io[g][k].min_density = mind;
 
-  /* LES sponge relaxation time per site (LBGKLESSpongeLayer::InitState). */
-  if (p->kernel == ORC_LBGKLES) {
+  /* Sponge relaxation time per site (LBGKLESSpongeLayer::InitState; the same in
+   * LBGKSpongeLayer.h:88-116 and TRTSpongeLayer.h:124-151). */
+  if (p->kernel == ORC_LBGKLES || p->kernel == ORC_LBGKSL || p->kernel == ORC_TRTSL) {
     s->vtau = (double*)malloc(sizeof(double) * (size_t)(n + 1));
     const double width = p->sponge_width, widthsq = width * width;
     for (int64_t i = 0; i < n; i++) {
@@ -848,6 +850,20 @@ static inline void pre_collision(const orc_sim* s, int64_t i, hydro_t* h) {
     } else {
       h->tau = tau_les;
     }
+  } else if (s->p.kernel == ORC_LBGKSL || s->p.kernel == ORC_TRTSL) {
+    /* CalculateTau (LBGKSpongeLayer.h:124-140, TRTSpongeLayer.h:157-172): the sponge
+     * time for the first half of its lifetime, then a linear return to tau0. */
+    const double tau0 = s->p.tau;
+    const uint64_t ts = s->t;
+    const uint64_t life = s->p.sponge_lifetime;
+    const double vt = s->vtau[i];
+    if (ts <= life / 2) {
+      h->tau = vt;
+    } else if (ts < life) {
+      h->tau = (tau0 - vt) * 2.0 / (double)life * (double)ts + (2.0 * vt - tau0);
+    } else {
+      h->tau = tau0;
+    }
   }
 }
 
@@ -861,6 +877,22 @@ static inline void collide(const orc_sim* s, const double* f, const double* fneq
     const double tp = s->p.tau;
     const double op = s->omega;
     const double tm = 0.5 + lambda / (tp - 0.5);
+    const double om = -1.0 / tm;
+    fpost[0] = f[0] + op * fneq[0];
+    for (int i = 0; i < Q; i++) {
+      const int ib = INV[i];
+      if (ib < i) continue;
+      const double sym = 0.5 * op * (fneq[i] + fneq[ib]);
+      const double asym = 0.5 * om * (fneq[i] - fneq[ib]);
+      fpost[i] = f[i] + sym + asym;
+      fpost[ib] = f[ib] + sym - asym;
+    }
+  } else if (s->p.kernel == ORC_TRTSL) {
+    /* TRTSpongeLayer::DoCollide (TRTSpongeLayer.h:86-115): the symmetric rate stays
+     * the global omega, the antisymmetric one follows the site's sponge tau. */
+    const double lambda = s->p.relaxation_parameter;
+    const double op = s->omega;
+    const double tm = 0.5 + lambda / (tau_site - 0.5);
     const double om = -1.0 / tm;
     fpost[0] = f[0] + op * fneq[0];
     for (int i = 0; i < Q; i++) {

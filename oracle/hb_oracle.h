@@ -19,7 +19,7 @@ extern "C" {
 enum { ORC_Q = 19 };
 
 /* Collision kernels (src/lb/kernels/LBGK.h, TRT.h, LBGKLESSpongeLayer.h). */
-enum { ORC_LBGK = 0, ORC_TRT = 1, ORC_LBGKLES = 2 };
+enum { ORC_LBGK = 0, ORC_TRT = 1, ORC_LBGKLES = 2, ORC_LBGKSL = 3, ORC_TRTSL = 4 };
 /* Wall streamers (SimpleBounceBackDelegate.h, BouzidiFirdaousLallemandDelegate.h, GuoZhengShiDelegate.h). */
 enum { ORC_SBB = 0, ORC_BFL = 1, ORC_GZS = 2 };
 /* Iolet streamers and iolet value sources. */

@@ -19,7 +19,7 @@ from . import case as case_mod
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libhboracle.so")
 
-KERNELS = {"LBGK": 0, "TRT": 1, "LBGKLESSL": 2}
+KERNELS = {"LBGK": 0, "TRT": 1, "LBGKLESSL": 2, "LBGKSL": 3, "TRTSL": 4}
 WALLS = {"SBB": 0, "BFL": 1, "GZS": 2}
 IOLET_KINDS = {"cosine": 0, "wk3": 1, "parabolic": 2, "wk2": 3, "file": 4, "file_velocity": 5, "womersley": 6}
 

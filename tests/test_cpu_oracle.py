@@ -187,3 +187,26 @@ def test_oracle_stress_caches(case_dir):
     assert np.allclose(tan[wn] + nor[wn], tr[wn], rtol=1e-12, atol=1e-18)
     # tangential to the wall up to the float normal's |n|^2 - 1 (~1e-7)
     assert np.allclose(np.sum(tan[wn] * nrm[wn], axis=1), 0.0, atol=1e-6 * np.max(np.abs(tr[wn])))
+
+
+@pytest.mark.parametrize("sponge,plain", [("LBGKSL", "LBGK"), ("TRTSL", "TRT")])
+def test_oracle_sponge_kernels(tmp_path, sponge, plain):
+    """With a viscosity ratio of one the sponge time is tau0 everywhere, and the
+    sponge-layer kernels (LBGKSpongeLayer.h, TRTSpongeLayer.h) reduce to the plain
+    ones bit for bit; with a ratio of ten they slow the flow near the outlet."""
+    from hemepure_b200 import vessels
+    v = vessels.Pipe(5, 24)
+    vessels.voxelise(v, str(tmp_path / "p.gmy"))
+    runs = {}
+    for name, ratio in (("one", 1.0), ("ten", 10.0)):
+        xml = str(tmp_path / f"{name}.xml")
+        vessels.write_case_xml(xml, "p.gmy", v, vessels.CaseUnits(tau=0.6), 80, [vessels.PressureBC(1.002)],
+                               [vessels.PressureBC(0.998)], relaxation_parameter=3.0 / 16.0,
+                               sponge={"viscosity_ratio": ratio, "width": 8.0, "lifetime": 60})
+        o = O.Simulation(xml, sponge, "SBB")
+        assert o.run(80) == 0
+        runs[name] = o.f()
+    ref = O.Simulation(str(tmp_path / "one.xml"), plain, "SBB")
+    assert ref.run(80) == 0
+    assert np.array_equal(runs["one"], ref.f())
+    assert not np.array_equal(runs["ten"], ref.f())
