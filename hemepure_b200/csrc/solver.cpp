@@ -192,7 +192,11 @@ void Solver::upload() {
   }
 
   // LES sponge relaxation time per site (LBGKLESSpongeLayer::InitState,
-  // src/lb/kernels/LBGKLESSpongeLayer.h:87-116), in storage order.
+  // src/lb/kernels/LBGKLESSpongeLayer.h:87-116), in storage order.  The
+  // reference subtracts the outlet position from the site's integer coordinates
+  // with Vector3D<site_t>::operator-, which converts the position to integers
+  // first by truncation (src/util/Vector3D.h:238-243,396), so the squared
+  // distance is an integer.
   if (is_sponge(opt_.kernel)) {
     std::vector<double> vt(n);
     const double width = p_.sponge_width, widthsq = width * width;
@@ -200,10 +204,10 @@ void Solver::upload() {
       const int x = L_.st2ref[s];
       double vr = 1.0;
       for (int k = 0; k < p_.n_outlets; k++) {
-        const double dx = (double)t_.coords[3 * x] - p_.outlets[k].position[0];
-        const double dy = (double)t_.coords[3 * x + 1] - p_.outlets[k].position[1];
-        const double dz = (double)t_.coords[3 * x + 2] - p_.outlets[k].position[2];
-        const double distsq = dx * dx + dy * dy + dz * dz;
+        const int64_t dx = (int64_t)t_.coords[3 * x] - (int64_t)p_.outlets[k].position[0];
+        const int64_t dy = (int64_t)t_.coords[3 * x + 1] - (int64_t)p_.outlets[k].position[1];
+        const int64_t dz = (int64_t)t_.coords[3 * x + 2] - (int64_t)p_.outlets[k].position[2];
+        const double distsq = (double)(dx * dx + dy * dy + dz * dz);
         const double dist = std::sqrt(distsq);
         if (distsq <= widthsq) vr *= 1.0 + (p_.viscosity_ratio - 1.0) * (dist / width - 1.0) * (dist / width - 1.0);
       }

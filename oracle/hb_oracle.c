@@ -759,17 +759,20 @@ int orc_sim_create(const orc_lattice* lat, const orc_params* p, orc_sim** out, c
     for (int k = 0; k < s->nio[g]; k++) s->io[g][k].min_density = mind;
 
   /* Sponge relaxation time per site (LBGKLESSpongeLayer::InitState; the same in
-   * LBGKSpongeLayer.h:88-116 and TRTSpongeLayer.h:124-151). */
+   * LBGKSpongeLayer.h:88-116 and TRTSpongeLayer.h:124-151).  `siteLocation -
+   * outletPositions[j]` is Vector3D<site_t>::operator-, whose argument is the
+   * position converted to integers by truncation (src/util/Vector3D.h:238-243,
+   * 396): the squared distance is an integer sum. */
   if (p->kernel == ORC_LBGKLES || p->kernel == ORC_LBGKSL || p->kernel == ORC_TRTSL) {
     s->vtau = (double*)malloc(sizeof(double) * (size_t)(n + 1));
     const double width = p->sponge_width, widthsq = width * width;
     for (int64_t i = 0; i < n; i++) {
       double vr = 1.0;
       for (int k = 0; k < p->n_outlets; k++) {
-        const double dx = (double)lat->coords[3 * i] - p->outlets[k].position[0];
-        const double dy = (double)lat->coords[3 * i + 1] - p->outlets[k].position[1];
-        const double dz = (double)lat->coords[3 * i + 2] - p->outlets[k].position[2];
-        const double distsq = dx * dx + dy * dy + dz * dz;
+        const int64_t dx = (int64_t)lat->coords[3 * i] - (int64_t)p->outlets[k].position[0];
+        const int64_t dy = (int64_t)lat->coords[3 * i + 1] - (int64_t)p->outlets[k].position[1];
+        const int64_t dz = (int64_t)lat->coords[3 * i + 2] - (int64_t)p->outlets[k].position[2];
+        const double distsq = (double)(dx * dx + dy * dy + dz * dz);
         const double dist = sqrt(distsq);
         if (distsq <= widthsq)
           vr *= 1.0 + (p->viscosity_ratio - 1.0) * (dist / width - 1.0) * (dist / width - 1.0);
