@@ -12,8 +12,15 @@ plain form does not shard, so there is no collective on the data path.
 Rank 0 prints one JSON line.  `value` is whole-job MLUPS (site updates per
 second over all ranks / 1e6) timed with CUDA events on the library's stream,
 max over ranks; `e2e` is the same metric measured through the C ABI one
-hb_step call at a time (each call uploads the step's iolet densities and
-reads back the stability word, with a host synchronisation).
+step at a time as a HemePure host drives it (the host hands over the step's
+pressure-iolet densities, hb_step(1) uploads the step's iolet row and reads
+back the stability word, with a host synchronisation).
+
+The CPU baseline and the reference arm (`--impl reference`) run HemePure's
+own code, compiled from its sources into oracle/_ref (single-rank: no MPI
+library exists on these machines), as one copy of the lattice per host core
+side by side, on a bounded number of steps; where those executables are not
+built, the oracle's C restatement runs on all host threads instead.
 """
 
 from __future__ import annotations
@@ -134,8 +141,38 @@ def make_workload(name: str, out_dir: str):
     return xml, info
 
 
+def reference_cpu(xml: str, kernel: str, wall: str, n_sites: int, budget_s: float, max_steps: int,
+                  warmup: int = 1):
+    """HemePure itself (compiled from its own sources, single-rank) on the host
+    cores: one copy of the lattice per core side by side, `warmup` untimed
+    steps each, then a bounded number of timed steps sized to about `budget_s`
+    seconds from a single-copy rate probe.  None when the executables are not
+    built on this machine."""
+    from oracle import reference as R
+    try:
+        combo = R.combo_for(xml, kernel, wall)
+    except (KeyError, ValueError):
+        return None
+    if not R.available(combo):
+        return None
+    probe = R.timed_replicas(xml, kernel, wall, 2, procs=1, warmup=0)
+    per_step_s = probe["span_s"] / 2
+    # Side by side the copies share memory bandwidth: 16 copies of the 4M-site
+    # pipe each step about 1.3x slower than one copy alone on the 16-core hosts.
+    steps = int(max(1, min(max_steps, budget_s / max(per_step_s * 1.5, 1e-6))))
+    r = R.timed_replicas(xml, kernel, wall, steps, warmup=warmup)
+    return {"value": r["MLUPS"], "unit": "MLUPS", "cores": r["procs"], "kind": "reference",
+            "cpu_model": r["cpu_model"],
+            "sample": f"HemePure's own code (single-rank build, {combo}) as {r['procs']} copies of the full "
+                      f"{r['sites']}-site lattice side by side, one per core, {warmup} untimed step(s) then "
+                      f"{r['steps']} timed steps each ({r['procs'] * r['sites'] * r['steps']} site updates over "
+                      f"{r['span_s']:.1f} s from the first copy's loop start to the last one's end)",
+            "single_copy_MLUPS": n_sites / per_step_s / 1e6}
+
+
 def cpu_baseline(xml: str, kernel: str, wall: str, n_sites: int, budget_s: float = 12.0, threads: int = 0):
-    """The oracle (the reference's algorithm restated in C) on the host cores."""
+    """The oracle (the reference's algorithm restated in C) on the host cores,
+    used when the reference's own executables are not built here."""
     from oracle import oracle as O
     threads = threads or os.cpu_count() or 1
     sim = O.Simulation(xml, kernel, wall, threads=threads)
@@ -215,26 +252,16 @@ def main():
               % (19 * n_sites * 8 / 1e9), "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
     if args.impl == "reference":
-        # The reference itself cannot be built here (it needs MPI, Boost and ParMETIS,
-        # which are absent); its algorithm runs as the C restatement on all host threads.
-        total_budget = 150.0
-        from oracle import oracle as O
-        threads = os.cpu_count() or 1
-        sim = O.Simulation(xml, kernel, wall, threads=threads)
-        t0 = time.perf_counter()
-        sim.run(1)
-        one = time.perf_counter() - t0
-        steps = int(max(1, min(args.steps, total_budget / max(one, 1e-6))))
-        t0 = time.perf_counter()
-        sim.run(steps)
-        dt = time.perf_counter() - t0
-        v = n_sites * steps / dt / 1e6
+        # HemePure itself, compiled from its own sources (oracle/_ref), one copy per
+        # host core; its C restatement on all host threads where it is not built.
+        base = reference_cpu(xml, kernel, wall, n_sites, budget_s=60.0, max_steps=args.steps, warmup=warmup)
+        if base is None:
+            base = cpu_baseline(xml, kernel, wall, n_sites, budget_s=120.0)
+        v = base["value"]
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": warmup, "ms_per_step": dt * 1e3 / steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
-                "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": threads, "kind": "port",
-                                 "sample": f"{steps} of {args.steps} requested time steps (bounded to ~{total_budget:.0f} s) "
-                                           f"of the full lattice after 1 warm-up step"},
+                "steps": args.steps, "warmup": warmup, "ms_per_step": n_sites / (v * 1e6) * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": config, "cpu_baseline": base,
                 "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -273,8 +300,8 @@ def main():
     prof_steps = 200
     s_ms, b_ms, g_ms = sim.profile_steps(prof_steps)
     from hemepure_b200.lbm import Geometry, read_case
-    p, gmy = read_case(xml, kernel)
-    lay = Geometry(gmy).layout(p, wall)
+    p_case, gmy = read_case(xml, kernel)
+    lay = Geometry(gmy).layout(p_case, wall)
     step_launch_ms = s_ms / prof_steps
     bulk_launch_ms = b_ms / prof_steps
     achieved = bytes_per_site * lay["bulk_sites"] / (bulk_launch_ms * 1e-3) / 1e9
@@ -294,18 +321,25 @@ def main():
                                   "achieved": bytes_per_site * n_sites / (step_launch_ms * 1e-3) / 1e9},
                 "whole_step_frac": (bytes_per_site * n_sites / (ms / args.steps * 1e-3) / 1e9) / peak}
 
-    # End to end through the C ABI: one hb_step call per step, host-synchronised.
+    # End to end through the C ABI, as a HemePure host drives it: per step the
+    # host's BoundaryValues hand over the pressure-iolet densities
+    # (hb_set_iolet_densities from host memory), hb_step(1) uploads that step's
+    # iolet row (96 doubles) and reads back the stability word, host-synchronised.
     e2e_steps = min(args.steps, 500)
+    din = np.ones(max(1, p_case.n_inlets))[:p_case.n_inlets]
+    dout = np.ones(max(1, p_case.n_outlets))[:p_case.n_outlets]
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
+        sim.SetIoletDensities(din, dout)
         sim.step(1)
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
+    sim.SetIoletDensities()
     e2e = {"value": world * n_sites * e2e_steps / e2e_s / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": 96 * 8,
            "d2h_bytes_per_step": 4, "steps": e2e_steps,
-           "note": "one hb_step(1) call per step: the step's iolet row (96 doubles, uploaded 1024 steps at a "
-                   "time), stability word down, host sync"}
+           "note": "per step: hb_set_iolet_densities (the outlet's density from host memory), hb_step(1) "
+                   "uploading that step's 96-double iolet row, 4-byte stability word read back, host sync"}
 
     # The shifted low-precision forms on the same lattice (same step count).
     forms = {"fp64": {"MLUPS": value / world, "bytes_per_site": 304,
@@ -334,7 +368,9 @@ def main():
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(xml, kernel, wall, n_sites)
+        base = reference_cpu(xml, kernel, wall, n_sites, budget_s=15.0, max_steps=args.steps)
+        if base is None:
+            base = cpu_baseline(xml, kernel, wall, n_sites)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,

@@ -395,13 +395,15 @@ void Solver::fill_density_rows(uint64_t t_first, int count) {
 }
 
 // The rows depend on the step alone (the Windkessel kernel rewrites its own
-// entries of a row at that row's step), so a window of 1024 precomputed rows
-// serves consecutive hb_step calls of any length with one upload: a caller that
-// steps one step per call no longer uploads a row each step.
-int Solver::density_row(uint64_t t) {
-  if (!rows_valid_ || t < rows_first_ || t >= rows_first_ + (uint64_t)dens_rows_) {
-    fill_density_rows(t, dens_rows_);
+// entries of a row at that row's step), so the rows a call needs are uploaded
+// together when it starts: up to 1024 rows for an hb_step call of many steps,
+// one row (768 bytes) for a call that advances one step.
+int Solver::density_row(uint64_t t, int64_t steps_ahead) {
+  if (!rows_valid_ || t < rows_first_ || t >= rows_first_ + (uint64_t)rows_count_) {
+    const int count = (int)std::max<int64_t>(1, std::min<int64_t>(steps_ahead, dens_rows_));
+    fill_density_rows(t, count);
     rows_first_ = t;
+    rows_count_ = count;
     rows_valid_ = true;
   }
   return (int)(t - rows_first_);
@@ -421,7 +423,7 @@ void Solver::set_iolet_densities(const double* inlets, int n_inlets, const doubl
 }
 
 void Solver::request_comms() {
-  if (!phase_open_) row_ = density_row(t_step_);
+  if (!phase_open_) row_ = density_row(t_step_, 1);
   launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
   phase_open_ = true;
 }
@@ -503,7 +505,7 @@ int Solver::step(int64_t nsteps, uint32_t flags) {
   const int per_step = (nwk3_ ? 1 : 0) + (L_.n > 0 ? 1 : 0) + (L_.G > 0 ? 1 : 0);
   check(cudaEventRecord(ev0_, stream_), "event");
   for (int64_t j = 0; j < nsteps; j++) {
-    row_ = density_row(t_step_);
+    row_ = density_row(t_step_, nsteps - j);
     phase_open_ = true;
     launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
     const bool macro = (flags & HB_STEP_MACRO) && (j == nsteps - 1);
@@ -532,7 +534,7 @@ int Solver::profile(int64_t nsteps, double ms[3]) {
   for (int pass = 0; pass < 2; pass++) {
     for (int64_t j = 0; j < nsteps; j++) {
       {
-        row_ = density_row(t_step_);
+        row_ = density_row(t_step_, nsteps - j);
         phase_open_ = true;
         launch_wk3_begin(wk3_.as<WK3Dev>(), nwk3_, cpl_buf_.as<double>(), dens_.as<double>() + (size_t)row_ * kRowStride, stream_);
         check(cudaEventRecord(e[0], stream_), "event");

@@ -83,7 +83,7 @@ class Solver {
   void fill_density_rows(uint64_t t_first, int count);
   // Index of step t's iolet row in the device table, refilling the table with
   // the rows of steps t .. t + 1023 when t lies outside the resident window.
-  int density_row(uint64_t t);
+  int density_row(uint64_t t, int64_t steps_ahead);
   StepArgs args() const;
   void check(cudaError_t e, const char* what);
   bool mixed() const { return opt_.precision != HB_STORE_FP64; }
@@ -118,6 +118,7 @@ class Solver {
   std::vector<double> host_rows_;
   bool rows_valid_ = false;         // the device table holds the rows of steps rows_first_ ...
   uint64_t rows_first_ = 0;
+  int rows_count_ = 0;              // rows uploaded at rows_first_
   bool dens_override_ = false;
   double dens_override_v_[32] = {};  // inlets 0-15, outlets 16-31
   int nwk3_ = 0;

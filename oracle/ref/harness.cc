@@ -8,11 +8,22 @@
 // and writes the distributions and the macroscopic caches of the last step to a
 // binary dump in the reference's contiguous site order.
 //
-// usage: hemepure_ref <config.xml> <output-dir> <steps> <dump-file> [threads-ignored]
+// usage: hemepure_ref <config.xml> <output-dir> <steps> <dump-file | -> [warm-up steps]
+//
+// Warm-up steps run before the timed loop (and before the start barrier below)
+// and count toward the step total.
 //
 // Dump layout (little-endian): char[8] "HBREFDMP", int64 n_sites, int64 steps_done,
 // int64 stability, then int64 coords[n][3], double f_old[n][19], double rho[n],
-// double u[n][3], double wss[n].
+// double u[n][3], double wss[n].  A dump file of "-" writes nothing (timing runs).
+//
+// For timing several copies side by side: with HB_REF_READY=<dir> set, the run
+// creates <dir>/ready.<pid> once set up and waits (at most ten minutes) for
+// <dir>/go before its first step.  The last stderr line gives the stepping
+// loop's start and end on CLOCK_MONOTONIC, comparable across processes.
+#include <time.h>
+#include <unistd.h>
+
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -46,6 +57,23 @@ namespace {
 
 typedef hemelb::lb::lattices::HEMELB_LATTICE Lattice;
 
+double monotonic() {
+  timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+// Start barrier between copies timed side by side (see the header comment).
+void wait_for_go() {
+  const char* dir = std::getenv("HB_REF_READY");
+  if (!dir || !*dir) return;
+  const std::string ready = std::string(dir) + "/ready." + std::to_string((long)getpid());
+  if (FILE* f = std::fopen(ready.c_str(), "w")) std::fclose(f);
+  const std::string go = std::string(dir) + "/go";
+  const double until = monotonic() + 600.0;
+  while (access(go.c_str(), F_OK) != 0 && monotonic() < until) usleep(1000);
+}
+
 template <class T>
 void put(FILE* f, const T* p, size_t n) {
   if (std::fwrite(p, sizeof(T), n, f) != n) {
@@ -62,6 +90,7 @@ int run(int argc, char** argv) {
   }
   const long steps = std::atol(argv[3]);
   const std::string dump = argv[4];
+  const long warmup = argc > 5 ? std::atol(argv[5]) : 0;
 
   net::MpiCommunicator commWorld = net::MpiCommunicator::World();
   net::IOCommunicator ioComms(commWorld);
@@ -115,8 +144,14 @@ int run(int argc, char** argv) {
   stepManager.RegisterCommsForAllPhases(netConcern);
 
   lb::MacroscopicPropertyCache& cache = lbm->GetPropertyCache();
+  for (long s = 0; s < warmup && simulationState->GetStability() != lb::Unstable; ++s) {
+    cache.ResetRequirements();
+    stepManager.CallActions();
+    simulationState->Increment();
+  }
   long done = 0;
-  double t0 = MPI_Wtime();
+  wait_for_go();
+  double t0 = monotonic();
   for (long s = 0; s < steps; ++s) {
     cache.ResetRequirements();
     if (s == steps - 1) {
@@ -129,12 +164,13 @@ int run(int argc, char** argv) {
     if (simulationState->GetStability() == lb::Unstable) break;
     simulationState->Increment();
   }
-  double t1 = MPI_Wtime();
+  double t1 = monotonic();
 
   const int64_t n = latticeData->GetLocalFluidSiteCount();
-  std::fprintf(stderr, "hemepure_ref: %lld sites, %ld steps, %.3f s, %.2f MLUPS\n", (long long)n, done,
-               t1 - t0, (double)n * (double)done / (t1 - t0) / 1e6);
+  std::fprintf(stderr, "hemepure_ref: %lld sites, %ld steps, %.3f s, loop %.6f %.6f, %.2f MLUPS\n", (long long)n,
+               done, t1 - t0, t0, t1, (double)n * (double)done / (t1 - t0) / 1e6);
 
+  if (dump == "-") return 0;
   FILE* out = std::fopen(dump.c_str(), "wb");
   if (!out) {
     std::perror(dump.c_str());

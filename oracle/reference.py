@@ -140,3 +140,93 @@ class Run:
 
     def __getitem__(self, key):
         return self.data[key]
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _mem_available_bytes() -> int:
+    try:
+        with open("/proc/meminfo") as fh:
+            for line in fh:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def timed_replicas(xml_path: str, kernel: str, wall: str, steps: int, procs: int = 0, bytes_per_site: int = 700,
+                   warmup: int = 1, timeout: float = 1800.0) -> Dict[str, object]:
+    """Aggregate throughput of HemePure on the host cores.
+
+    The reference is built single-rank here (there is no MPI library on these
+    machines), so the host's cores are used by `procs` independent copies of the
+    same lattice run side by side, one process per core: every copy reads and
+    sets up the case and runs `warmup` untimed steps, all wait at a common
+    start barrier, then each steps `steps` times.  The result is all copies'
+    site updates over the span from the first loop start to the last loop end.
+    Every copy does the per-site work of an MPI rank over the same cores
+    without its halo exchange.  `procs` defaults to the
+    core count, capped so the copies fit in half the available memory
+    (`bytes_per_site` per copy and site: two FP64 distribution arrays, the
+    64-bit neighbour table and the site data)."""
+    combo = combo_for(xml_path, kernel, wall)
+    exe = binary(combo)
+    if not os.access(exe, os.X_OK):
+        raise FileNotFoundError(f"{exe} is not built")
+    root = ET.parse(xml_path).getroot()
+    cores = os.cpu_count() or 1
+    work = tempfile.mkdtemp(prefix="hemepure_ref_rep_")
+    try:
+        # Site count from a one-step probe (also warms the page cache for the geometry).
+        probe = subprocess.run([exe, os.path.abspath(xml_path), os.path.join(work, "probe"), "1", "-"],
+                               cwd=os.path.dirname(os.path.abspath(xml_path)), capture_output=True, text=True,
+                               timeout=timeout)
+        if probe.returncode != 0:
+            raise RuntimeError(f"hemepure_ref failed: {probe.stderr[-2000:]}")
+        n_sites = int(probe.stderr.strip().splitlines()[-1].split()[1])
+        if procs <= 0:
+            mem = _mem_available_bytes()
+            fit = max(1, int(0.5 * mem // max(1, n_sites * bytes_per_site))) if mem else cores
+            procs = max(1, min(cores, fit))
+        ready = os.path.join(work, "sync")
+        os.makedirs(ready)
+        env = dict(os.environ, HB_REF_READY=ready)
+        ps = [subprocess.Popen([exe, os.path.abspath(xml_path), os.path.join(work, f"o{i}"), str(int(steps)), "-",
+                                str(int(warmup))],
+                               cwd=os.path.dirname(os.path.abspath(xml_path)), env=env,
+                               stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True)
+              for i in range(procs)]
+        t_end = time.monotonic() + timeout
+        while len([f for f in os.listdir(ready) if f.startswith("ready.")]) < procs:
+            if any(p.poll() not in (None, 0) for p in ps) or time.monotonic() > t_end:
+                for p in ps:
+                    p.kill()
+                raise RuntimeError("a reference copy failed before the start barrier")
+            time.sleep(0.01)
+        open(os.path.join(ready, "go"), "w").close()
+        starts, ends = [], []
+        for p in ps:
+            _, err = p.communicate(timeout=max(1.0, t_end - time.monotonic()))
+            if p.returncode != 0:
+                raise RuntimeError(f"hemepure_ref failed: {err[-2000:]}")
+            words = err.strip().splitlines()[-1].replace(",", " ").split()
+            k = words.index("loop")
+            starts.append(float(words[k + 1]))
+            ends.append(float(words[k + 2]))
+        span = max(ends) - min(starts)
+        return {"MLUPS": procs * n_sites * steps / span / 1e6, "procs": procs, "sites": n_sites, "steps": steps,
+                "warmup": warmup,
+                "span_s": span, "per_copy_s": [e - s for s, e in zip(starts, ends)], "combo": combo,
+                "cpu_model": cpu_model()}
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
