@@ -28,7 +28,7 @@
 namespace hb {
 namespace {
 
-constexpr int kGeneralBlocksPerSM = 8;
+constexpr int kGeneralBlocksPerSM = 5;
 
 // ---------------------------------------------------------------------------
 // Kernels
@@ -47,11 +47,13 @@ __global__ void __launch_bounds__(256, (is_sponge(K) || MACRO) ? 1 : 3) k_bulk(c
   bulk_site_f64<K, GATHER, MACRO>(a, s, r);
 }
 
-// The boundary kernel is latency-bound: with LBGK or TRT, bounce-back or BFL
-// walls and no outputs it is held to 64 registers so that 16 warps per SM hide
-// its dependent loads (it spills a little; LBGK/BFL measured 20% faster than at
-// 94 registers, and the whole step 5% faster).  The sponge-layer kernels, GZS walls and
-// output steps, which would spill far more, keep the compiler's allocation.
+// The boundary kernel is latency-bound.  Its gather issues the eighteen loads
+// of a record together (f64_site.cuh), which needs the registers to hold them:
+// with LBGK or TRT, bounce-back or BFL walls and no outputs it is held to 96
+// registers, five blocks of 128 per SM (4M-site pipe, time alone: 64 registers
+// 0.0628 ms with spills, 80 registers 0.0571 ms, 96 registers 0.0553 ms; the
+// whole step 0.2298 / 0.2231 / 0.2215 ms).  The sponge-layer kernels, GZS walls
+// and output steps keep the compiler's allocation.
 template <int K, int WALL, bool GATHER, bool MACRO>
 __global__ void __launch_bounds__(128, (!is_sponge(K) && WALL != kGZS && !MACRO) ? kGeneralBlocksPerSM : 1)
     k_general(const StepArgs a) {
