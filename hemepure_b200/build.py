@@ -26,9 +26,10 @@ CU_SOURCES = {
     "noalloc.cu": [],
     "kernels_batch.cu": [],
     "gmy_device.cu": [],
+    "shard.cu": [],
 }
-CPP_SOURCES = ["xml.cpp", "config.cpp", "layout.cpp", "solver.cpp", "extraction.cpp", "batch.cpp", "capi.cpp"]
-HEADERS = ["hb_common.h", "f64_site.cuh", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h", "mixed_site.cuh", "batch.h", "batch_dev.h"]
+CPP_SOURCES = ["xml.cpp", "config.cpp", "layout.cpp", "shard.cpp", "solver.cpp", "extraction.cpp", "batch.cpp", "capi.cpp"]
+HEADERS = ["hb_common.h", "f64_site.cuh", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h", "mixed_site.cuh", "batch.h", "batch_dev.h", "shard.h"]
 
 
 def _deps_mtime() -> float:
@@ -36,8 +37,28 @@ def _deps_mtime() -> float:
     return max(os.path.getmtime(p) for p in paths if os.path.exists(p))
 
 
+def _local_includes(path: str, seen: set) -> None:
+    """The quoted #include files of `path` within the source tree, transitively."""
+    if path in seen or not os.path.exists(path):
+        return
+    seen.add(path)
+    with open(path) as fh:
+        for line in fh:
+            t = line.strip()
+            if t.startswith("#include") and '"' in t:
+                inc = t.split('"')[1]
+                _local_includes(os.path.normpath(os.path.join(os.path.dirname(path), inc)), seen)
+
+
 def _stale(src: str, obj: str, hdr_mtime: float) -> bool:
-    return not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src), hdr_mtime)
+    """An object is stale when it is older than its source, one of the source's
+    own headers (followed through quoted includes) or this script."""
+    if not os.path.exists(obj):
+        return True
+    deps: set = set()
+    _local_includes(src, deps)
+    newest = max([os.path.getmtime(d) for d in deps] + [os.path.getmtime(__file__)])
+    return os.path.getmtime(obj) < newest
 
 
 def _run(cmd):

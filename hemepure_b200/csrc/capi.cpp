@@ -1,5 +1,6 @@
 // capi.cpp -- the extern "C" boundary (include/hemeb200.h).  No C++ exception
 // crosses it: every entry point catches and returns an HB_* status.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <memory>
@@ -10,6 +11,7 @@
 #include "config.h"
 #include "extraction.h"
 #include "solver.h"
+#include "shard.h"
 
 struct hb_handle {
   std::unique_ptr<hb::Solver> solver;
@@ -104,6 +106,104 @@ int hb_create_from_xml(const char* xml_path, const hb_options* opt, hb_handle** 
   });
 }
 
+int hb_shard_plan(const char* xml_path, int kernel, int n_shards, int* axis, int64_t* bounds) {
+  if (!xml_path || !axis || !bounds || n_shards < 1) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    hb::CaseConfig c = hb::read_case(xml_path, kernel);
+    hb::LatticeTables t = hb::read_gmy(c.gmy_path);
+    const std::vector<int64_t> b = hb::plan_slabs(t, n_shards, axis);
+    std::copy(b.begin(), b.end(), bounds);
+    return HB_OK;
+  });
+}
+
+int hb_create_shard_from_xml(const char* xml_path, const hb_options* opt, const hb_shard* shard, hb_handle** out) {
+  if (!xml_path || !shard || !out) return HB_ERR_ARG;
+  *out = nullptr;
+  return guard(nullptr, [&] {
+    hb_options o;
+    hb_default_options(&o);
+    if (opt) o = *opt;
+    hb::CaseConfig c = hb::read_case(xml_path, o.kernel);
+    if (!c.checkpoint_file.empty())
+      throw hb::Error{HB_ERR_UNSUPPORTED, "a shard starts from the equilibrium: set its distributions with hb_set_fs"};
+    hb::LatticeTables full = o.geometry_reader == HB_GEOMETRY_DEVICE ? hb::read_gmy_device(c.gmy_path, o.device)
+                                                                      : hb::read_gmy(c.gmy_path);
+    hb::LatticeTables t = hb::cut_shard(full, c.params, shard->axis, shard->lo, shard->hi);
+    full = hb::LatticeTables();
+    int rc = finish_create(std::move(t), c.params, o, out);
+    if (rc != HB_OK) return rc;
+    try {
+      (*out)->solver->attach_shard(shard->axis, shard->lo, shard->hi);
+    } catch (...) {
+      delete *out;
+      *out = nullptr;
+      throw;
+    }
+    (*out)->solver->set_units(c.dt, c.dx, c.origin);
+    return HB_OK;
+  });
+}
+
+int hb_shard_halo_sizes(const hb_handle* h, int64_t counts[4], int* elem_bytes) {
+  if (!h || !counts) return HB_ERR_ARG;
+  if (!h->solver->sharded()) return HB_ERR_ARG;
+  h->solver->shard_sizes(counts);
+  if (elem_bytes) *elem_bytes = h->solver->elem_size();
+  return HB_OK;
+}
+
+int hb_shard_pack(hb_handle* h, void* to_lower, void* to_upper, void* stream) {
+  if (!h) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->shard_pack(to_lower, to_upper, static_cast<cudaStream_t>(stream));
+    return HB_OK;
+  });
+}
+
+int hb_shard_unpack(hb_handle* h, const void* from_lower, const void* from_upper, void* stream) {
+  if (!h) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->shard_unpack(from_lower, from_upper, static_cast<cudaStream_t>(stream));
+    return HB_OK;
+  });
+}
+
+int hb_shard_site_ids(const hb_handle* h, int64_t* ids) {
+  if (!h || !ids) return HB_ERR_ARG;
+  const hb::LatticeTables& t = h->solver->tables();
+  const int64_t n = t.owned();
+  for (int64_t k = 0; k < n; k++) ids[k] = t.gid.empty() ? k : t.gid[k];
+  return HB_OK;
+}
+
+int hb_shard_describe(const char* xml_path, int kernel, int wall, const hb_shard* shard, int64_t counts[6],
+                      int64_t* owned, int64_t* halo, int64_t* send_lower, int64_t* send_upper, int64_t* recv_lower,
+                      int64_t* recv_upper) {
+  if (!xml_path || !shard || !counts) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    hb::CaseConfig c = hb::read_case(xml_path, kernel);
+    hb::LatticeTables full = hb::read_gmy(c.gmy_path);
+    hb::LatticeTables t = hb::cut_shard(full, c.params, shard->axis, shard->lo, shard->hi);
+    const hb::Layout L = hb::build_layout(t, c.params, wall);
+    const hb::HaloLists hl = hb::halo_lists(t, L, shard->axis, shard->lo, shard->hi);
+    const int64_t no = t.owned();
+    counts[0] = no;
+    counts[1] = t.n - no;
+    counts[2] = (int64_t)hl.send[0].size();
+    counts[3] = (int64_t)hl.send[1].size();
+    counts[4] = (int64_t)hl.recv[0].size();
+    counts[5] = (int64_t)hl.recv[1].size();
+    if (owned) std::copy(t.gid.begin(), t.gid.begin() + no, owned);
+    if (halo) std::copy(t.gid.begin() + no, t.gid.end(), halo);
+    int64_t* lists[4] = {send_lower, send_upper, recv_lower, recv_upper};
+    const std::vector<int64_t>* src[4] = {&hl.send_pairs[0], &hl.send_pairs[1], &hl.recv_pairs[0], &hl.recv_pairs[1]};
+    for (int k = 0; k < 4; k++)
+      if (lists[k]) std::copy(src[k]->begin(), src[k]->end(), lists[k]);
+    return HB_OK;
+  });
+}
+
 int hb_create(const hb_lattice_desc* lat, const hb_params* params, const hb_options* opt, hb_handle** out) {
   if (!lat || !params || !out || lat->n_sites <= 0 || !lat->coords || !lat->wall_mask || !lat->iolet_mask ||
       !lat->site_type || !lat->iolet_id)
@@ -183,7 +283,7 @@ int hb_step(hb_handle* h, int64_t n_steps, uint32_t flags) {
 
 int hb_site_count(const hb_handle* h, int64_t* n) {
   if (!h || !n) return HB_ERR_ARG;
-  *n = h->solver->tables().n;
+  *n = h->solver->tables().owned();  // a shard's own sites, without its halo
   return HB_OK;
 }
 
@@ -267,8 +367,16 @@ int hb_get_tables(const hb_handle* h, int64_t* neighbours, uint32_t* wall_mask, 
   if (!h) return HB_ERR_ARG;
   return guard(nullptr, [&] {
     const hb::LatticeTables& t = h->solver->tables();
-    const size_t n = (size_t)t.n;
-    if (neighbours) hb::neighbour_table(t, neighbours);
+    const size_t n = (size_t)t.owned();
+    if (neighbours) {
+      if ((int64_t)n == t.n) {
+        hb::neighbour_table(t, neighbours);
+      } else {  // a shard: its own sites' rows, indices in the shard's numbering (halo sites after the owned ones)
+        std::vector<int64_t> all((size_t)t.n * hb::Q);
+        hb::neighbour_table(t, all.data());
+        std::memcpy(neighbours, all.data(), n * hb::Q * sizeof(int64_t));
+      }
+    }
     if (wall_mask) std::memcpy(wall_mask, t.wall.data(), n * sizeof(uint32_t));
     if (iolet_mask) std::memcpy(iolet_mask, t.iolet.data(), n * sizeof(uint32_t));
     if (site_type) std::memcpy(site_type, t.stype.data(), n * sizeof(int32_t));

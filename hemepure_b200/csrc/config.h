@@ -54,6 +54,13 @@ struct LatticeTables {
   std::vector<float> normal;        // [n*3] wall normal, normalised in float (HUGE_VALF without one)
   std::vector<int64_t> nbr;         // [n*19] neighbourIndices, or empty: derived from the coordinates
                                     // when asked for (neighbour_table)
+  // One slab of a sharded lattice: sites [0, n_owned) are this shard's own, in
+  // the reference's order; sites [n_owned, n) are halo sites of the neighbouring
+  // slabs, whose post-collision values arrive every step.  -1: all sites owned.
+  int64_t n_owned = -1;
+  std::vector<int64_t> gid;         // [n] global contiguous index of each site (shards only)
+
+  int64_t owned() const { return n_owned >= 0 ? n_owned : n; }
 
   int collision_type(int64_t i) const {
     const bool w = wall[i] != 0;

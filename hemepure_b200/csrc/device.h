@@ -124,6 +124,10 @@ constexpr int kSumSitesPerBlock = 2048;
 int moment_sum_blocks(int64_t n);
 void launch_moment_sums(const double* f, int64_t dir_stride, int64_t site_stride, int64_t n, double* scratch,
                         double* out, void* stream);
+// Sharded form (shard.cu): out[k] = f[idx[k]] and f[idx[k]] = in[k] over m
+// stored elements of `elem_bytes` bytes (8 FP64, 4 FP32, 2 FP16 storage).
+void launch_halo_pack(const void* f, const int64_t* idx, int64_t m, void* out, int elem_bytes, void* stream);
+void launch_halo_unpack(const void* in, const int64_t* idx, int64_t m, void* f, int elem_bytes, void* stream);
 // AoS reference order <-> SoA storage order.
 void launch_soa_to_aos_f64(const double* soa, int64_t np, const int* st2ref, int n, double* aos, void* stream);
 void launch_aos_to_soa_f64(const double* aos, const int* st2ref, int n, double* soa, int64_t np, void* stream);

@@ -175,7 +175,7 @@ V3f normalised(V3f v) {  // Vector3D::GetNormalised (util/Vector3D.h:270-292)
 }  // namespace
 
 std::vector<uint8_t> select_sites(const LatticeTables& t, const hb_selector& sel, double voxel, const double origin[3]) {
-  const int64_t n = t.n;
+  const int64_t n = t.owned();  // a shard selects among its own sites
   std::vector<uint8_t> mask((size_t)n, 0);
   if (sel.type < HB_SELECT_WHOLE || sel.type > HB_SELECT_SURFACE_POINT) throw Error{HB_ERR_ARG, "unknown geometry selector"};
   // Selector state as the reference's constructors hold it: float vectors and radii.
@@ -249,8 +249,8 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
   std::vector<uint8_t> take;
   if (sel) take = select_sites(t, *sel, s.dx(), s.origin());
   int64_t n_out = 0;
-  for (int64_t i = 0; i < t.n; i++) n_out += (!sel || take[(size_t)i]) ? 1 : 0;
-  const int64_t n = t.n;
+  const int64_t n = t.owned();
+  for (int64_t i = 0; i < n; i++) n_out += (!sel || take[(size_t)i]) ? 1 : 0;
   if (s.time_step() <= 1) throw Error{HB_ERR_ARG, "no completed time step to write"};
   const uint64_t label = s.time_step() - 1;
   bool need_macro = false, need_f = false;
@@ -418,7 +418,7 @@ void read_checkpoint(Solver& s, const std::string& path, uint64_t step) {
   const double offset = x.f64();
   if (name != "distributions" || nf != (uint32_t)Q) throw Error{HB_ERR_FORMAT, "checkpoint field is not 'distributions' of 19 values"};
   const LatticeTables& t = s.tables();
-  if ((int64_t)nsites != t.n) throw Error{HB_ERR_FORMAT, "checkpoint site count differs from the lattice"};
+  if ((int64_t)nsites != t.owned()) throw Error{HB_ERR_FORMAT, "checkpoint site count differs from the lattice"};
   const size_t hdr = x.pos;
   const size_t reclen = 8 + (size_t)nsites * (12 + 4 * Q);
   if ((buf.size() - hdr) % reclen != 0) throw Error{HB_ERR_FORMAT, "Checkpoint file length not consistent with integer number of checkpoints"};
@@ -445,8 +445,8 @@ void read_checkpoint(Solver& s, const std::string& path, uint64_t step) {
   }
   XdrIn r{buf.data() + hdr + idx * reclen, reclen};
   const uint64_t label = r.u64();
-  std::vector<double> f((size_t)t.n * Q);
-  for (int64_t i = 0; i < t.n; i++) {
+  std::vector<double> f((size_t)t.owned() * Q);
+  for (int64_t i = 0; i < t.owned(); i++) {
     const uint32_t px = r.u32(), py = r.u32(), pz = r.u32();
     if ((int64_t)px != t.coords[3 * i] || (int64_t)py != t.coords[3 * i + 1] || (int64_t)pz != t.coords[3 * i + 2])
       throw Error{HB_ERR_FORMAT, "Site read at index " + std::to_string(i) + " does not match the lattice's site order"};

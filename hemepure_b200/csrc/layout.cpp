@@ -84,19 +84,23 @@ struct PassError {
 
 Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
   Layout L;
-  const int64_t n64 = t.n;
+  // Sites [n, nt) of a shard's tables are halo sites: stored after the owned
+  // sites, never updated, their pushes into owned sites recorded as pulls.
+  const int64_t nt64 = t.n;
+  const int64_t n64 = t.owned();
   if (n64 <= 0) throw Error{HB_ERR_ARG, "lattice has no fluid sites"};
-  if (n64 > (int64_t)1 << 30) throw Error{HB_ERR_UNSUPPORTED, "more than 2^30 sites in one lattice"};
-  const int n = (int)n64;
+  if (nt64 > (int64_t)1 << 30) throw Error{HB_ERR_UNSUPPORTED, "more than 2^30 sites in one lattice"};
+  const int n = (int)n64, nt = (int)nt64;
   L.n = n;
-  L.np = ((n64 + 63) / 64) * 64;
+  L.n_halo = nt - n;
+  L.np = ((nt64 + 63) / 64) * 64;
   const int64_t D[3] = {t.dims[0], t.dims[1], t.dims[2]};
   PassError err;
 
   // Dense grid of reference indices.
   std::vector<int32_t> grid(D[0] * D[1] * D[2], -1);
   auto gidx = [&](int64_t x, int64_t y, int64_t z) { return (x * D[1] + y) * D[2] + z; };
-  parallel_for(n, [&](int64_t b, int64_t e) {
+  parallel_for(nt, [&](int64_t b, int64_t e) {
     for (int64_t i = b; i < e; i++) {
       const int64_t* c = &t.coords[3 * i];
       if (c[0] < 0 || c[1] < 0 || c[2] < 0 || c[0] >= D[0] || c[1] >= D[1] || c[2] >= D[2]) {
@@ -114,12 +118,18 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
   err.raise();
   // neighbourIndices[x*19 + d]: the tables' own when they carry one, else from the grid
   // (LatticeData::InitialiseNeighbourLookup).
+  // (For a shard the rubbish slot is nt * Q.)
   auto neighbour = [&](int x, int d) -> int64_t {
     if (!t.nbr.empty()) return t.nbr[(size_t)x * Q + d];
     const int64_t px = t.coords[3 * x] + cx(d), py = t.coords[3 * x + 1] + cy(d), pz = t.coords[3 * x + 2] + cz(d);
-    if (px < 0 || py < 0 || pz < 0 || px >= D[0] || py >= D[1] || pz >= D[2]) return n64 * Q;
+    if (px < 0 || py < 0 || pz < 0 || px >= D[0] || py >= D[1] || pz >= D[2]) return nt64 * Q;
     const int32_t g = grid[gidx(px, py, pz)];
-    return g >= 0 ? (int64_t)g * Q + d : n64 * Q;
+    return g >= 0 ? (int64_t)g * Q + d : nt64 * Q;
+  };
+  // An owned site at these coordinates (runs join owned sites only).
+  auto owned_at = [&](const int64_t* c) {
+    const int32_t g = grid[gidx(c[0], c[1], c[2])];
+    return g >= 0 && g < n;
   };
 
   // Run axis: fewest sites whose predecessor along the axis is not fluid.
@@ -131,7 +141,7 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
       for (int64_t i = b; i < e; i++) {
         int64_t c[3] = {t.coords[3 * i], t.coords[3 * i + 1], t.coords[3 * i + 2]};
         c[a] -= 1;
-        if (c[a] < 0 || grid[gidx(c[0], c[1], c[2])] < 0) r++;
+        if (c[a] < 0 || !owned_at(c)) r++;
       }
       runs += r;
     });
@@ -145,7 +155,8 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
   // Storage order: rows along a0, ordered by (c[a2], c[a1]): the grid read in
   // that order.  A site starts a run when its predecessor along a0 is not fluid.
   L.st2ref.resize(n);
-  L.ref2st.resize(n);
+  L.ref2st.resize(nt);
+  for (int x = n; x < nt; x++) L.ref2st[x] = x;  // halo sites keep their order after the owned ones
   std::vector<int> run_of(n);
   {
     const int64_t R = D[a2] * D[a1];  // rows
@@ -155,7 +166,8 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
       c[a2] = row / D[a1];
       c[a1] = row % D[a1];
       c[a0] = k;
-      return grid[gidx(c[0], c[1], c[2])];
+      const int32_t g = grid[gidx(c[0], c[1], c[2])];
+      return g < n ? g : -1;
     };
     parallel_for(R, [&](int64_t b, int64_t e) {
       for (int64_t row = b; row < e; row++) {
@@ -200,26 +212,29 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
     std::fill(src.get() + b, src.get() + e, -1);
     std::fill(writers.get() + b, writers.get() + e, (uint8_t)0);
   });
-  parallel_for(n, [&](int64_t b, int64_t e) {
+  parallel_for(nt, [&](int64_t b, int64_t e) {
     for (int64_t xx = b; xx < e; xx++) {
       const int x = (int)xx;
       const int ct = t.collision_type(x);
       const int sx = L.ref2st[x];
+      const bool halo = x >= n;
       for (int d = 0; d < Q; d++) {
         const bool io = d > 0 && ct >= 2 && ((t.iolet[x] >> (d - 1)) & 1u);
         const bool wl = d > 0 && (ct == 1 || ct >= 4) && ((t.wall[x] >> (d - 1)) & 1u);
         if (io || wl) {
+          if (halo) continue;  // a halo site's own delegates are the other shard's
           const size_t slot = (size_t)sx * Q + inv(d);
           __atomic_fetch_add(&writers[slot], (uint8_t)1, __ATOMIC_RELAXED);
           src[slot] = -2;
         } else {
           const int64_t target = neighbour(x, d);
-          if (target == n64 * Q) continue;  // the rubbish slot
-          if (target < 0 || target > n64 * Q || target % Q != d) {
+          if (target == nt64 * Q) continue;  // the rubbish slot
+          if (target < 0 || target > nt64 * Q || target % Q != d) {
             err.set(HB_ERR_BAD_INDEX, "neighbour index out of range or in the wrong direction");
             return;
           }
           const int y = (int)(target / Q);
+          if (y >= n) continue;  // into a halo site: the other shard's slot
           const size_t slot = (size_t)L.ref2st[y] * Q + d;
           __atomic_fetch_add(&writers[slot], (uint8_t)1, __ATOMIC_RELAXED);
           src[slot] = sx;
@@ -250,7 +265,7 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
       for (int s = run_start[r]; s < run_start[r + 1]; s++)
         for (int i = 1; i < Q; i++) {
           const int v = src[(size_t)s * Q + i];
-          if (v >= 0 && !((set >> i) & 1u)) {
+          if (v >= 0 && v < n && !((set >> i) & 1u)) {
             off[i] = v - s;
             set |= 1u << i;
           }
@@ -265,7 +280,7 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
       for (int i = 1; i < Q; i++) {
         const int v = src[(size_t)s * Q + i];
         if (v < 0) all_bulk = false;
-        else if (v - s != off[i]) ok = false;
+        else if (v >= n || v - s != off[i]) ok = false;  // pulls from a halo site follow no run
       }
       regular[s] = ok;
       plain[s] = ok && all_bulk && t.collision_type(L.st2ref[s]) == 0;
@@ -352,6 +367,8 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
         const double q = t.q[(size_t)18 * x + d - 1];
         if (q < 0.75 && !bi && !bw && src[(size_t)s * Q + d] < 0)
           throw Error{HB_ERR_UNSUPPORTED, "GZS wall link without a fluid neighbour behind the site"};
+        if (q < 0.75 && !bi && !bw && src[(size_t)s * Q + d] >= n)
+          throw Error{HB_ERR_UNSUPPORTED, "GZS wall link whose extrapolation neighbour lies in another shard"};
       }
     }
   }
@@ -371,7 +388,7 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
     c.count = (int)v.size();
     for (auto& pr : v) L.g_cpl[pr.second] = slot++;
     const hb_iolet& io = iolet_cfg(idx);
-    for (int i = 0; i < n; i++) {
+    for (int i = 0; i < n; i++) {  // owned sites only: a shard holds its own centre or none
       bool in = true;
       for (int k = 0; k < 3; k++) {
         const double cc = (double)t.coords[3 * i + k];

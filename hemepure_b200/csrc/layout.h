@@ -11,8 +11,9 @@
 namespace hb {
 
 struct Layout {
-  int n = 0;
-  int64_t np = 0;                 // padded stride of one direction plane
+  int n = 0;                      // sites updated here (a shard's own sites)
+  int n_halo = 0;                 // halo sites of a shard, stored at [n, n + n_halo)
+  int64_t np = 0;                 // padded stride of one direction plane (covers the halo sites)
   int axis = 2;                   // run axis
   std::vector<int> st2ref, ref2st;
   std::vector<int> meta;          // [n]

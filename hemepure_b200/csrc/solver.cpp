@@ -9,6 +9,7 @@
 //                  gathers (kernels_f64.cu)
 //   EndIteration   swap the two buffers, time step + 1
 #include "solver.h"
+#include "shard.h"
 
 #include <algorithm>
 #include <cmath>
@@ -118,6 +119,7 @@ Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& 
 
 Solver::~Solver() {
   if (stream_) cudaStreamSynchronize(stream_);
+  if (xev_) cudaEventDestroy(xev_);
   if (side_) cudaStreamSynchronize(side_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
@@ -501,6 +503,8 @@ int Solver::read_status() {
 
 int Solver::step(int64_t nsteps, uint32_t flags) {
   if (nsteps < 0) throw Error{HB_ERR_ARG, "negative step count"};
+  if (shard_ && nsteps > 1)
+    throw Error{HB_ERR_ARG, "a shard advances one step per call: its halo is exchanged between steps"};
   int64_t launches = 0;
   const int per_step = (nwk3_ ? 1 : 0) + (L_.n > 0 ? 1 : 0) + (L_.G > 0 ? 1 : 0);
   check(cudaEventRecord(ev0_, stream_), "event");
@@ -749,6 +753,58 @@ void Solver::get_wk3(int group, int index, double st[4]) {
     return;
   }
   throw Error{HB_ERR_ARG, "iolet is not a Windkessel iolet"};
+}
+
+}  // namespace hb
+
+namespace hb {
+
+void Solver::attach_shard(int axis, int64_t lo, int64_t hi) {
+  const HaloLists h = halo_lists(t_, L_, axis, lo, hi);
+  int64_t tot = 0;
+  for (int side = 0; side < 2; side++) {
+    send_n_[side] = (int64_t)h.send[side].size();
+    recv_n_[side] = (int64_t)h.recv[side].size();
+    upload_vec(send_idx_[side], h.send[side].empty() ? std::vector<int64_t>{0} : h.send[side], tot);
+    upload_vec(recv_idx_[side], h.recv[side].empty() ? std::vector<int64_t>{0} : h.recv[side], tot);
+  }
+  dev_bytes_ += tot;
+  check(cudaEventCreateWithFlags(&xev_, cudaEventDisableTiming), "cudaEventCreate");
+  shard_ = true;
+}
+
+void Solver::shard_sizes(int64_t counts[4]) const {
+  counts[0] = send_n_[0];
+  counts[1] = send_n_[1];
+  counts[2] = recv_n_[0];
+  counts[3] = recv_n_[1];
+}
+
+void Solver::shard_pack(void* to_lower, void* to_upper, cudaStream_t caller) {
+  if (!shard_) throw Error{HB_ERR_ARG, "not a shard"};
+  if ((send_n_[0] && !to_lower) || (send_n_[1] && !to_upper)) throw Error{HB_ERR_ARG, "missing send buffer"};
+  // The buffer holding the last step's post-collision values (direct mode: the
+  // values set by hb_set_fs, which the neighbours' first step does not read).
+  const void* f = f_[cur_].p;
+  void* out[2] = {to_lower, to_upper};
+  for (int side = 0; side < 2; side++)
+    if (send_n_[side]) launch_halo_pack(f, send_idx_[side].as<int64_t>(), send_n_[side], out[side], (int)elem_bytes(), stream_);
+  check(cudaGetLastError(), "halo pack");
+  check(cudaEventRecord(xev_, stream_), "event");
+  if (caller && caller != stream_) check(cudaStreamWaitEvent(caller, xev_, 0), "stream wait");
+}
+
+void Solver::shard_unpack(const void* from_lower, const void* from_upper, cudaStream_t caller) {
+  if (!shard_) throw Error{HB_ERR_ARG, "not a shard"};
+  if ((recv_n_[0] && !from_lower) || (recv_n_[1] && !from_upper)) throw Error{HB_ERR_ARG, "missing receive buffer"};
+  if (caller && caller != stream_) {
+    check(cudaEventRecord(xev_, caller), "event");
+    check(cudaStreamWaitEvent(stream_, xev_, 0), "stream wait");
+  }
+  const void* in[2] = {from_lower, from_upper};
+  for (int side = 0; side < 2; side++)
+    if (recv_n_[side]) launch_halo_unpack(in[side], recv_idx_[side].as<int64_t>(), recv_n_[side], f_[cur_].p, (int)elem_bytes(), stream_);
+  check(cudaGetLastError(), "halo unpack");
 }
 
 }  // namespace hb

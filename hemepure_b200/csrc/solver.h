@@ -76,6 +76,18 @@ class Solver {
   bool get_previous_fs(double* f);
   void set_time_step(uint64_t t) { t_step_ = t; }
 
+  // Sharded form (tables cut by cut_shard): the halo lists of the slab
+  // [lo, hi) along `axis`; then, after every step, pack the values the two
+  // neighbours pull and, before the next, unpack theirs.  Both run on the
+  // solver's stream, ordered against the caller's stream by events.
+  void attach_shard(int axis, int64_t lo, int64_t hi);
+  bool sharded() const { return shard_; }
+  // Elements sent to the lower / upper neighbour, received from them.
+  void shard_sizes(int64_t counts[4]) const;
+  int elem_size() const { return (int)elem_bytes(); }
+  void shard_pack(void* to_lower, void* to_upper, cudaStream_t caller);
+  void shard_unpack(const void* from_lower, const void* from_upper, cudaStream_t caller);
+
  private:
   void upload();
   void materialise();
@@ -138,6 +150,11 @@ class Solver {
   bool prev_direct_ = false;
   double dt_ = 1.0, dx_ = 1.0;
   double origin_[3] = {0, 0, 0};
+  // Sharded form.
+  bool shard_ = false;
+  int64_t send_n_[2] = {0, 0}, recv_n_[2] = {0, 0};
+  DeviceBuffer send_idx_[2], recv_idx_[2];
+  cudaEvent_t xev_ = nullptr;
 };
 
 }  // namespace hb

@@ -49,6 +49,8 @@ EXPORTS = [
     "hb_batch_stats",
     "hb_batch_prepare_xml", "hb_batch_prep_sites", "hb_batch_add_prepared", "hb_batch_prep_free",
     "hb_write_xtr_selected", "hb_geometry_select", "hb_read_case_iolet_table", "hb_iolet_velocity",
+    "hb_shard_plan", "hb_create_shard_from_xml", "hb_shard_halo_sizes", "hb_shard_pack", "hb_shard_unpack",
+    "hb_shard_site_ids", "hb_shard_describe",
     "hb_geometry_open_device", "hb_geometry_read_timing",
 ]
 
@@ -181,6 +183,13 @@ def library() -> C.CDLL:
     L.hb_batch_prep_sites.argtypes = [P, P]
     L.hb_batch_add_prepared.argtypes = [P, P, P]
     L.hb_batch_prep_free.argtypes = [P]
+    L.hb_shard_plan.argtypes = [C.c_char_p, I, I, P, P]
+    L.hb_create_shard_from_xml.argtypes = [C.c_char_p, P, P, C.POINTER(P)]
+    L.hb_shard_halo_sizes.argtypes = [P, P, P]
+    L.hb_shard_pack.argtypes = [P, P, P, P]
+    L.hb_shard_unpack.argtypes = [P, P, P, P]
+    L.hb_shard_site_ids.argtypes = [P, P]
+    L.hb_shard_describe.argtypes = [C.c_char_p, I, I, P, P, P, P, P, P, P, P]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name != "hb_default_options":
@@ -191,6 +200,17 @@ def library() -> C.CDLL:
 
 def _p(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
+
+
+def check_rc(rc: int, what: str) -> None:
+    """Raise HemeLBError for a failed call that takes no handle."""
+    if rc != HB_OK:
+        raise HemeLBError(rc, f"{what}: {last_create_error()}")
+
+
+def _dptr(t) -> Optional[int]:
+    """Device pointer of a torch tensor (or None)."""
+    return None if t is None else int(t.data_ptr())
 
 
 GEOMETRY_READERS = {"host": 0, "device": 1}
@@ -216,11 +236,18 @@ class LBM:
 
     def __init__(self, xml_path: Optional[str] = None, kernel: str = "LBGK", wall: str = "SBB",
                  precision: str = "fp64", device: int = 0, lattice: Optional[Dict[str, np.ndarray]] = None,
-                 params: Optional[Params] = None, geometry_reader: str = "device"):
+                 params: Optional[Params] = None, geometry_reader: str = "device", shard=None):
+        """`shard` = (axis, lo, hi): only the slab lo <= coordinate < hi of the
+        case's lattice, with its halo (hb_create_shard_from_xml)."""
         L = library()
         self._h = C.c_void_p()
         self._opt = options(kernel, wall, precision, device, geometry_reader)
-        if xml_path is not None:
+        if shard is not None:
+            from .shard import ShardSpec
+            spec = ShardSpec(int(shard[0]), int(shard[1]), int(shard[2]))
+            rc = L.hb_create_shard_from_xml(os.fspath(xml_path).encode(), C.byref(self._opt), C.byref(spec),
+                                            C.byref(self._h))
+        elif xml_path is not None:
             rc = L.hb_create_from_xml(os.fspath(xml_path).encode(), C.byref(self._opt), C.byref(self._h))
         else:
             if lattice is None or params is None:
@@ -398,6 +425,31 @@ class LBM:
         n = C.c_int64()
         library().hb_last_step_timing(self._h, C.byref(ms), C.byref(n))
         return float(ms.value), int(n.value)
+
+    # -- sharded form -------------------------------------------------------------------
+    def shard_halo_sizes(self):
+        """Stored elements (send lower, send upper, receive lower, receive upper)
+        and the element size in bytes."""
+        c = np.zeros(4, np.int64)
+        e = C.c_int()
+        self._check(library().hb_shard_halo_sizes(self._h, _p(c), C.byref(e)))
+        return [int(v) for v in c], int(e.value)
+
+    def shard_pack(self, to_lower, to_upper, stream: Optional[int] = None) -> None:
+        """Device tensors (or raw device pointers) of the send buffers."""
+        lo = to_lower if isinstance(to_lower, (int, type(None))) else _dptr(to_lower)
+        hi = to_upper if isinstance(to_upper, (int, type(None))) else _dptr(to_upper)
+        self._check(library().hb_shard_pack(self._h, lo, hi, stream))
+
+    def shard_unpack(self, from_lower, from_upper, stream: Optional[int] = None) -> None:
+        lo = from_lower if isinstance(from_lower, (int, type(None))) else _dptr(from_lower)
+        hi = from_upper if isinstance(from_upper, (int, type(None))) else _dptr(from_upper)
+        self._check(library().hb_shard_unpack(self._h, lo, hi, stream))
+
+    def shard_site_ids(self) -> np.ndarray:
+        ids = np.zeros(self.n, np.int64)
+        self._check(library().hb_shard_site_ids(self._h, _p(ids)))
+        return ids
 
     def profile_steps(self, n: int):
         """Advance 2n steps timing the launches: (step launch ms over the first n

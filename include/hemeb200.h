@@ -176,8 +176,61 @@ int hb_post_receive(hb_handle* h);
 /* LBM::EndIteration + SimulationState::Increment. */
 int hb_end_iteration(hb_handle* h);
 
-/* All phases of `n_steps` time steps; HB_STEP_MACRO fills the caches on the last. */
+/* All phases of `n_steps` time steps; HB_STEP_MACRO fills the caches on the last.
+ * A shard (below) advances one step per call. */
 int hb_step(hb_handle* h, int64_t n_steps, uint32_t flags);
+
+/* ---- one lattice over several GPUs: slabs with a halo exchange --------------
+ * The reference decomposes a lattice over MPI ranks
+ * (src/geometry/decomposition/BasicDecomposition.cc:42-64, refined by
+ * OptimisedDecomposition) and every step sends the post-collision values of
+ * the links crossing into another rank and copies the received ones into place
+ * (LatticeData::SendAndReceive / CopyReceived, src/geometry/LatticeData.cc:665-689).
+ * Here the lattice is cut into slabs across one axis, one per GPU.  A shard
+ * handle owns its slab's sites and keeps the fluid sites of the plane beyond
+ * each cut as halo sites.  After each hb_step(h, 1, ...) the caller packs the
+ * values its two neighbours pull (hb_shard_pack), exchanges the buffers with
+ * them (for example NCCL send/recv), and unpacks what it received
+ * (hb_shard_unpack) before the next step.  Each list is ordered by (global
+ * site index, direction), so neighbouring shards agree on it without talking.
+ * The arithmetic of every site is the single-lattice arithmetic: the shards
+ * together give the single-lattice results bit for bit.  Rejected with
+ * HB_ERR_UNSUPPORTED: a GZS wall link whose extrapolation neighbour is a halo
+ * site, and a Windkessel iolet whose sites or centre site span two slabs. */
+typedef struct hb_shard {
+  int axis;       /* 0, 1 or 2: the axis the cuts cross */
+  int64_t lo, hi; /* this shard owns the sites with lo <= coordinate < hi */
+} hb_shard;
+
+/* Slab bounds with balanced site counts for n_shards shards: shard k owns
+ * [bounds[k], bounds[k+1]); *axis < 0 on entry picks the axis with the largest
+ * extent of fluid sites (the axis is returned).  bounds has n_shards + 1 entries.
+ * Plays the role of BasicDecomposition::Decompose for slabs. */
+int hb_shard_plan(const char* xml_path, int kernel, int n_shards, int* axis, int64_t* bounds);
+/* hb_create_from_xml for one shard. */
+int hb_create_shard_from_xml(const char* xml_path, const hb_options* opt, const hb_shard* shard, hb_handle** out);
+/* Stored elements sent to the lower / upper neighbour and received from them
+ * per step: counts[0] send lower, [1] send upper, [2] receive lower, [3]
+ * receive upper; *elem_bytes: 8 (FP64), 4 (FP32) or 2 (FP16 storage). */
+int hb_shard_halo_sizes(const hb_handle* h, int64_t counts[4], int* elem_bytes);
+/* After a step: the values the neighbours pull, into device buffers of
+ * counts[0] and counts[1] elements (NULL where the count is 0).  Ordered after
+ * the step on the handle's stream; `stream` (a cudaStream_t, or NULL) is made to
+ * wait for the pack, so work queued on it afterwards sees the buffers filled. */
+int hb_shard_pack(hb_handle* h, void* to_lower, void* to_upper, void* stream);
+/* Before the next step: the neighbours' values into the halo sites.  The unpack
+ * waits for the work queued so far on `stream` (where the receives completed). */
+int hb_shard_unpack(hb_handle* h, const void* from_lower, const void* from_upper, void* stream);
+/* Global contiguous index of each owned site, in the handle's reference order
+ * (the order of hb_get_fs and hb_get_macro), [n]. */
+int hb_shard_site_ids(const hb_handle* h, int64_t* ids);
+/* The same shard described on the host, with no GPU: counts[0] owned sites,
+ * [1] halo sites, [2..5] entries of the send-lower, send-upper, receive-lower and
+ * receive-upper lists; owned / halo: global indices; each list: (global site
+ * index, direction) pairs in exchange order.  Any output pointer may be NULL. */
+int hb_shard_describe(const char* xml_path, int kernel, int wall, const hb_shard* shard, int64_t counts[6],
+                      int64_t* owned, int64_t* halo, int64_t* send_lower, int64_t* send_upper, int64_t* recv_lower,
+                      int64_t* recv_upper);
 
 /* ---- state access ---------------------------------------------------------- */
 
@@ -378,9 +431,13 @@ int hb_geometry_close(hb_geometry* g);
  * NULL).  Nothing is allocated: the scratch is a fixed 256 KiB array in the
  * library, so one call takes at most 16,777,216 sites (more returns HB_ERR_ARG).
  * The first call on a device looks up that array's device address (once per
- * device); make it before any stream capture.  Calls share the array, so two
- * calls whose kernels overlap on one GPU race; the result is ready when
- * `stream` is synchronised.  Errors: hb_last_error(NULL, ...). */
+ * device, again after a device reset replaced the device's context); make it
+ * before any stream capture.  Under CUDA's lazy module loading (the default)
+ * the array is created on a device when the library's module loads there, at
+ * the latest by that first call: a caller that commits all its device memory
+ * makes one warm-up call before.  Calls share the array, so two calls whose
+ * kernels overlap on one GPU race; the result is ready when `stream` is
+ * synchronised.  Errors: hb_last_error(NULL, ...). */
 int hb_moment_sums_noalloc(const double* f, int64_t dir_stride, int64_t site_stride, int64_t n_sites, double* sums,
                            void* stream);
 
