@@ -27,6 +27,9 @@ CU_SOURCES = {
     "kernels_batch.cu": [],
     "gmy_device.cu": [],
     "shard.cu": [],
+    "layout_device.cu": [],
+    # the selectors' float arithmetic as the host rounds it
+    "extract.cu": ["-fmad=false"],
 }
 CPP_SOURCES = ["xml.cpp", "config.cpp", "layout.cpp", "shard.cpp", "solver.cpp", "extraction.cpp", "batch.cpp", "capi.cpp"]
 HEADERS = ["hb_common.h", "f64_site.cuh", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h", "mixed_site.cuh", "batch.h", "batch_dev.h", "shard.h"]

@@ -253,7 +253,7 @@ void Batch::clear_member_tables(const BatchMember& m) {
   check(cudaStreamSynchronize(stream_), "clear");
 }
 
-std::unique_ptr<PreparedLattice> prepare_lattice(LatticeTables t, const hb_params& p, int kernel, int wall, uint64_t steps) {
+void validate_batch_case(const hb_params& p, int kernel, int wall) {
   if (kernel != kLBGK && kernel != kTRT) throw Error{HB_ERR_UNSUPPORTED, "the batched form runs LBGK or TRT"};
   if (wall != kSBB && wall != kBFL) throw Error{HB_ERR_UNSUPPORTED, "the batched form runs bounce-back or BFL walls"};
   for (int k = 0; k < p.n_inlets + p.n_outlets; k++) {
@@ -262,9 +262,15 @@ std::unique_ptr<PreparedLattice> prepare_lattice(LatticeTables t, const hb_param
       throw Error{HB_ERR_UNSUPPORTED, "the batched form runs cosine pressure and parabolic velocity iolets"};
   }
   if (!(p.tau > 0.5)) throw Error{HB_ERR_ARG, "tau must exceed 1/2"};
+}
+
+std::unique_ptr<PreparedLattice> prepare_lattice(LatticeTables t, const hb_params& p, int kernel, int wall, uint64_t steps,
+                                                 Layout* layout) {
+  validate_batch_case(p, kernel, wall);
   if (wall == kBFL && t.q.empty()) throw Error{HB_ERR_ARG, "BFL walls need wall distances"};
   auto prep = std::make_unique<PreparedLattice>();
-  prep->L = build_layout(t, p, wall);
+  if (layout) prep->L = std::move(*layout);
+  else prep->L = build_layout(t, p, wall);
   prep->t = std::move(t);
   prep->p = p;
   prep->kernel = kernel;
@@ -424,6 +430,7 @@ void Batch::capture(int k) {
   base.n = (int)sites_hw;
   base.meta = meta_.as<int>();
   base.run_off = run_off_.as<int>();
+  base.run_po = nullptr;
   base.gen.G = (int)cap_gen_;
   base.gen.site = g_site_.as<int>();
   base.gen.run = g_run_.as<int>();

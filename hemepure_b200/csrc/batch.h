@@ -45,7 +45,11 @@ struct PreparedLattice {
 };
 
 // Host-only: validate the physics the batched form supports and build the layout.
-std::unique_ptr<PreparedLattice> prepare_lattice(LatticeTables t, const hb_params& p, int kernel, int wall, uint64_t steps);
+// The checks of a batched case that need no lattice; throws hb::Error.
+void validate_batch_case(const hb_params& p, int kernel, int wall);
+// `layout`, when given, is the layout already built for these tables (moved from).
+std::unique_ptr<PreparedLattice> prepare_lattice(LatticeTables t, const hb_params& p, int kernel, int wall, uint64_t steps,
+                                                 Layout* layout = nullptr);
 
 struct BatchMember {
   int slot = -1;

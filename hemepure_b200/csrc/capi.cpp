@@ -50,9 +50,10 @@ int guard(hb_handle* h, F&& fn) {
   }
 }
 
-int finish_create(hb::LatticeTables t, const hb_params& p, const hb_options& o, hb_handle** out) {
+int finish_create(hb::LatticeTables t, const hb_params& p, const hb_options& o, hb_handle** out,
+                  hb::Layout* layout = nullptr) {
   auto h = std::make_unique<hb_handle>();
-  h->solver = std::make_unique<hb::Solver>(std::move(t), p, o);
+  h->solver = std::make_unique<hb::Solver>(std::move(t), p, o, layout);
   *out = h.release();
   return HB_OK;
 }
@@ -83,9 +84,13 @@ int hb_create_from_xml(const char* xml_path, const hb_options* opt, hb_handle** 
     hb_default_options(&o);
     if (opt) o = *opt;
     hb::CaseConfig c = hb::read_case(xml_path, o.kernel);
-    hb::LatticeTables t = o.geometry_reader == HB_GEOMETRY_DEVICE ? hb::read_gmy_device(c.gmy_path, o.device)
-                                                                   : hb::read_gmy(c.gmy_path);
-    int rc = finish_create(std::move(t), c.params, o, out);
+    // The device reader also lays the lattice out on the device.
+    hb::Layout L;
+    const bool dev = o.geometry_reader == HB_GEOMETRY_DEVICE;
+    if (dev) hb::validate_case(c.params, o);
+    hb::LatticeTables t = dev ? hb::read_gmy_device(c.gmy_path, o.device, nullptr, &c.params, o.wall, &L)
+                              : hb::read_gmy(c.gmy_path);
+    int rc = finish_create(std::move(t), c.params, o, out, dev ? &L : nullptr);
     if (rc == HB_OK) (*out)->solver->set_units(c.dt, c.dx, c.origin);
     if (rc == HB_OK && !c.checkpoint_file.empty()) {
       std::string cp = c.checkpoint_file;
@@ -103,6 +108,22 @@ int hb_create_from_xml(const char* xml_path, const hb_options* opt, hb_handle** 
       }
     }
     return rc;
+  });
+}
+
+int hb_write_state(hb_handle* h, const char* path) {
+  if (!h || !path) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->write_state(path);
+    return HB_OK;
+  });
+}
+
+int hb_read_state(hb_handle* h, const char* path) {
+  if (!h || !path) return HB_ERR_ARG;
+  return guard(h, [&] {
+    h->solver->read_state(path);
+    return HB_OK;
   });
 }
 
@@ -494,6 +515,22 @@ int hb_batch_prepare_xml(const char* xml_path, int kernel, int wall, uint64_t st
   });
 }
 
+int hb_batch_prepare_xml_device(const char* xml_path, int kernel, int wall, uint64_t steps, int device,
+                                hb_batch_prep** out) {
+  if (!xml_path || !out) return HB_ERR_ARG;
+  *out = nullptr;
+  return guard(nullptr, [&] {
+    hb::CaseConfig c = hb::read_case(xml_path, kernel);
+    hb::validate_batch_case(c.params, kernel, wall);
+    hb::Layout L;
+    hb::LatticeTables t = hb::read_gmy_device(c.gmy_path, device, nullptr, &c.params, wall, &L);
+    auto h = std::make_unique<hb_batch_prep>();
+    h->prep = hb::prepare_lattice(std::move(t), c.params, kernel, wall, steps, &L);
+    *out = h.release();
+    return HB_OK;
+  });
+}
+
 int hb_batch_prep_sites(const hb_batch_prep* prep, int64_t* sites) {
   if (!prep || !sites || !prep->prep) return HB_ERR_ARG;
   *sites = prep->prep->L.n;
@@ -690,6 +727,16 @@ int hb_geometry_layout(const hb_geometry* g, const hb_params* params, int wall, 
     stats[1] = L.runs;
     stats[2] = L.bulk_sites;
     stats[3] = L.G;
+    return HB_OK;
+  });
+}
+
+int hb_geometry_layout_digest(const hb_geometry* g, const hb_params* params, int wall, int device, uint64_t digest[32]) {
+  if (!g || !params || !digest) return HB_ERR_ARG;
+  return guard(nullptr, [&] {
+    const hb::Layout L = device < 0 ? hb::build_layout(g->tables, *params, wall)
+                                    : hb::build_layout_on_device(g->tables, *params, wall, device);
+    hb::layout_digest(L, digest);
     return HB_OK;
   });
 }

@@ -94,6 +94,10 @@ void build_neighbours(LatticeTables& t);
 struct GmyTiming {
   double read_ms = 0, inflate_ms = 0, h2d_ms = 0, device_ms = 0, d2h_ms = 0;
 };
-LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* timing = nullptr);
+// With `layout`, the storage layout for `params` and `wall` is built on the
+// device from the decoded tables while they are copied back to the host.
+struct Layout;
+LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* timing = nullptr,
+                              const hb_params* params = nullptr, int wall = 0, Layout* layout = nullptr);
 
 }  // namespace hb

@@ -65,6 +65,7 @@ struct StepArgs {
   int n;
   const int* meta;
   const int* run_off;
+  const int* run_po;      // [runs][20] plane offsets i * np + run_off[run][i] (shifted forms' bulk kernel), or null
   GeneralDev gen;
   // kernel parameters
   double tau, omega, omega_minus;
@@ -124,6 +125,27 @@ constexpr int kSumSitesPerBlock = 2048;
 int moment_sum_blocks(int64_t n);
 void launch_moment_sums(const double* f, int64_t dir_stride, int64_t site_stride, int64_t n, double* scratch,
                         double* out, void* stream);
+// Extraction on the device (extract.cu): a geometry selector evaluated per site
+// in the reference's order, in the reference selectors' float arithmetic.
+struct SelectArgs {
+  int64_t n;
+  const int32_t* coords;   // [n*3] lattice coordinates, reference order
+  const uint8_t* wall;     // [n] 1 for a site with a wall link
+  const uint8_t* stype;    // [n] 0 fluid, 1 inlet, 2 outlet
+  double voxel, origin[3];
+  int type;                // HB_SELECT_*
+  float point[3], normal[3], line[3];
+  float radius, line_len, max_surface_dist;
+};
+int select_blocks(int64_t n);
+// mask[n] and the selected indices in reference order into idx (*total of them);
+// counts needs select_blocks(n) ints.
+void launch_select(const SelectArgs& s, uint8_t* mask, int* counts, int* total, int* idx, void* stream);
+// out[k*width + j] = src[j*stride + ref2st[idx[k]]] for k < m (a field in storage order).
+void launch_gather_selected(const double* src, int64_t stride, int width, const int* idx, const int* ref2st, int m,
+                            double* out, void* stream);
+// out[k*width + j] = aos[idx[k]*width + j] (rows of an array in reference order).
+void launch_gather_rows(const double* aos, int width, const int* idx, int m, double* out, void* stream);
 // Sharded form (shard.cu): out[k] = f[idx[k]] and f[idx[k]] = in[k] over m
 // stored elements of `elem_bytes` bytes (8 FP64, 4 FP32, 2 FP16 storage).
 void launch_halo_pack(const void* f, const int64_t* idx, int64_t m, void* out, int elem_bytes, void* stream);

@@ -174,6 +174,20 @@ V3f normalised(V3f v) {  // Vector3D::GetNormalised (util/Vector3D.h:270-292)
 
 }  // namespace
 
+void selector_state(const hb_selector& sel, SelectArgs* a) {
+  if (sel.type < HB_SELECT_WHOLE || sel.type > HB_SELECT_SURFACE_POINT) throw Error{HB_ERR_ARG, "unknown geometry selector"};
+  const V3f point = to_f(sel.point), point2 = to_f(sel.point2);
+  const V3f normal = normalised(to_f(sel.normal));
+  const V3f line = sub(point2, point);
+  a->type = sel.type;
+  a->point[0] = point.x, a->point[1] = point.y, a->point[2] = point.z;
+  a->normal[0] = normal.x, a->normal[1] = normal.y, a->normal[2] = normal.z;
+  a->line[0] = line.x, a->line[1] = line.y, a->line[2] = line.z;
+  a->radius = (float)sel.radius;
+  a->line_len = mag(line);
+  a->max_surface_dist = (float)std::sqrt(3.0);
+}
+
 std::vector<uint8_t> select_sites(const LatticeTables& t, const hb_selector& sel, double voxel, const double origin[3]) {
   const int64_t n = t.owned();  // a shard selects among its own sites
   std::vector<uint8_t> mask((size_t)n, 0);
@@ -246,38 +260,53 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
   std::vector<std::string> names;
   const std::vector<std::string> fields = split_fields(fields_csv, &names);
   const LatticeTables& t = s.tables();
-  std::vector<uint8_t> take;
-  if (sel) take = select_sites(t, *sel, s.dx(), s.origin());
-  int64_t n_out = 0;
   const int64_t n = t.owned();
-  for (int64_t i = 0; i < n; i++) n_out += (!sel || take[(size_t)i]) ? 1 : 0;
   if (s.time_step() <= 1) throw Error{HB_ERR_ARG, "no completed time step to write"};
   const uint64_t label = s.time_step() - 1;
-  bool need_macro = false, need_f = false;
-  std::vector<double> stress[6];
+  bool need_macro = false, need_f = false, need_stress[6] = {false, false, false, false, false, false};
   for (auto& f : fields) {
     if (f == "distributions") need_f = true;
     else if (f == "pressure" || f == "velocity" || f == "shearstress") need_macro = true;
     const int sf = stress_field(f);
-    if (sf >= 0 && stress[sf].empty()) {
+    if (sf >= 0) need_stress[sf] = true;
+  }
+  // Data per written site k (row k of each array), and the written sites'
+  // indices in reference order.  With a selector, the sites are selected and
+  // their data gathered on the device, and only they are downloaded.
+  std::vector<int> idx;
+  std::vector<double> rho, u, wss, fd;
+  std::vector<double> stress[6];
+  if (sel) {
+    Solver::Selection got = s.select(*sel, need_macro, need_stress, need_f);
+    idx = std::move(got.idx);
+    rho = std::move(got.rho);
+    u = std::move(got.u);
+    wss = std::move(got.wss);
+    fd = std::move(got.fd);
+    for (int k = 0; k < 6; k++) stress[k] = std::move(got.stress[k]);
+  } else {
+    idx.resize(n);
+    for (int64_t i = 0; i < n; i++) idx[i] = (int)i;
+    for (int k = 0; k < 6; k++) {
+      if (!need_stress[k]) continue;
       if (!s.stress_valid())
         throw Error{HB_ERR_ARG, "the last step did not fill the stress caches (pass HB_STEP_MACRO | HB_STEP_STRESS)"};
-      stress[sf].resize((size_t)n * field_len(f));
-      s.get_stress(sf, stress[sf].data());
+      stress[k].resize((size_t)n * Solver::stress_len(k));
+      s.get_stress(k, stress[k].data());
+    }
+    if (need_macro) {
+      if (!s.macro_valid()) throw Error{HB_ERR_ARG, "the last step did not fill the macroscopic caches (pass HB_STEP_MACRO)"};
+      rho.resize(n);
+      u.resize(3 * n);
+      wss.resize(n);
+      s.get_macro(rho.data(), u.data(), wss.data());
+    }
+    if (need_f) {
+      fd.resize((size_t)n * Q);
+      if (!s.get_previous_fs(fd.data())) throw Error{HB_ERR_ARG, "the distributions of the last step are no longer held"};
     }
   }
-  std::vector<double> rho, u, wss, fd;
-  if (need_macro) {
-    if (!s.macro_valid()) throw Error{HB_ERR_ARG, "the last step did not fill the macroscopic caches (pass HB_STEP_MACRO)"};
-    rho.resize(n);
-    u.resize(3 * n);
-    wss.resize(n);
-    s.get_macro(rho.data(), u.data(), wss.data());
-  }
-  if (need_f) {
-    fd.resize((size_t)n * Q);
-    if (!s.get_previous_fs(fd.data())) throw Error{HB_ERR_ARG, "the distributions of the last step are no longer held"};
-  }
+  const int64_t n_out = (int64_t)idx.size();
 
   // Unit conversion (src/util/UnitConverter.cc, UnitConverter.h:61-119).
   const double dx = s.dx(), dt = s.dt();
@@ -314,11 +343,11 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
   }
   XdrOut rec;
   rec.u64(label);
-  for (int64_t i = 0; i < n; i++) {
-    if (sel && !take[(size_t)i]) continue;
-    rec.u32((uint32_t)t.coords[3 * i]);
-    rec.u32((uint32_t)t.coords[3 * i + 1]);
-    rec.u32((uint32_t)t.coords[3 * i + 2]);
+  for (int64_t i = 0; i < n_out; i++) {
+    const int64_t x = idx[i];  // the site's index in reference order; i is its row in the data arrays
+    rec.u32((uint32_t)t.coords[3 * x]);
+    rec.u32((uint32_t)t.coords[3 * x + 1]);
+    rec.u32((uint32_t)t.coords[3 * x + 2]);
     for (auto& f : fields) {
       if (f == "pressure") {
         const double p = rho[i] * kCs2;
@@ -350,7 +379,7 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
         const double* tr = &stress[HB_STRESS_TRACTION][(size_t)i * 3];
         const double scale = lattice_speed * lattice_speed * 1000.0;
         for (int k = 0; k < 3; k++) {
-          const double nk = (double)normal[(size_t)3 * i + k];
+          const double nk = (double)normal[(size_t)3 * x + k];
           rec.f32((float)(tr[k] * scale - nk * kRefPressureMmHg * kMmHgToPascal));
         }
       } else if (f == "tangentialprojectiontraction" || f == "normalprojectiontraction") {

@@ -35,10 +35,12 @@
 #include <chrono>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <thread>
 #include <vector>
 
 #include "config.h"
+#include "layout.h"
 
 namespace hb {
 namespace {
@@ -285,7 +287,9 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 
 }  // namespace
 
-LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* timing) {
+LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* timing, const hb_params* params, int wall,
+                              Layout* layout) {
+  if (layout && !params) throw Error{HB_ERR_ARG, "the layout needs the case parameters"};
   auto t0 = std::chrono::steady_clock::now();
   GmyTiming tm{};
   std::ifstream in(path, std::ios::binary);
@@ -337,12 +341,14 @@ LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* ti
 
   // Inflate on a pool of host threads.
   auto t1 = std::chrono::steady_clock::now();
-  std::vector<unsigned char> raw((size_t)std::max<int64_t>(raw_total, 16));
+  // Left uninitialised: the inflating threads touch its pages first, in parallel.
+  const size_t raw_size = (size_t)std::max<int64_t>(raw_total, 16);
+  std::unique_ptr<unsigned char[]> raw(new unsigned char[raw_size]);
   std::atomic<int> next{0}, failed{-1};
   auto work = [&]() {
     for (int k = next++; k < nb; k = next++) {
       uLongf dl = blocks[k].raw_len;
-      if (uncompress(raw.data() + blocks[k].raw_off, &dl, buf.data() + src_off[k], src_len[k]) != Z_OK) {
+      if (uncompress(raw.get() + blocks[k].raw_off, &dl, buf.data() + src_off[k], src_len[k]) != Z_OK) {
         int exp = -1;
         failed.compare_exchange_strong(exp, k);
         continue;
@@ -367,9 +373,9 @@ LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* ti
   } sg{st};
   Pool P;
   auto t2 = std::chrono::steady_clock::now();
-  uint32_t* d_raw = P.get<uint32_t>(raw.size() / 4 + 1);
+  uint32_t* d_raw = P.get<uint32_t>(raw_size / 4 + 1);
   BlockDev* d_blocks = P.get<BlockDev>(nb);
-  cuda_check(cudaMemcpyAsync(d_raw, raw.data(), raw.size(), cudaMemcpyHostToDevice, st), "copy of the inflated blocks");
+  cuda_check(cudaMemcpyAsync(d_raw, raw.get(), raw_size, cudaMemcpyHostToDevice, st), "copy of the inflated blocks");
   cuda_check(cudaMemcpyAsync(d_blocks, blocks.data(), sizeof(BlockDev) * nb, cudaMemcpyHostToDevice, st), "copy of the block table");
   cuda_check(cudaStreamSynchronize(st), "copy of the inflated blocks");
   tm.h2d_ms = ms_since(t2);
@@ -436,21 +442,64 @@ LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* ti
 
   auto t4 = std::chrono::steady_clock::now();
   t.n = n;
-  t.coords.resize(3 * (size_t)n);
-  t.wall.resize(n);
-  t.iolet.resize(n);
-  t.stype.resize(n);
-  t.iolet_id.resize(n);
-  t.q.resize(18 * (size_t)n);
-  t.normal.resize(3 * (size_t)n);
-  cuda_check(cudaMemcpyAsync(t.coords.data(), T.coords, t.coords.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
-  cuda_check(cudaMemcpyAsync(t.wall.data(), T.wall, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "D2H");
-  cuda_check(cudaMemcpyAsync(t.iolet.data(), T.iolet, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "D2H");
-  cuda_check(cudaMemcpyAsync(t.stype.data(), T.stype, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "D2H");
-  cuda_check(cudaMemcpyAsync(t.iolet_id.data(), T.iolet_id, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "D2H");
-  cuda_check(cudaMemcpyAsync(t.q.data(), T.q, t.q.size() * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
-  cuda_check(cudaMemcpyAsync(t.normal.data(), T.normal, t.normal.size() * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
-  cuda_check(cudaStreamSynchronize(st), "copy of the tables");
+  // The tables come back to the host on a second stream and host thread while
+  // the layout's passes (when asked for) run on the device copy.
+  cudaStream_t st2;
+  cuda_check(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking), "cudaStreamCreate");
+  StreamGuard sg2{st2};
+  cudaError_t d2h_err = cudaSuccess;
+  auto download = [&]() {
+    try {
+      t.coords.resize(3 * (size_t)n);
+      t.wall.resize(n);
+      t.iolet.resize(n);
+      t.stype.resize(n);
+      t.iolet_id.resize(n);
+      t.q.resize(18 * (size_t)n);
+      t.normal.resize(3 * (size_t)n);
+    } catch (const std::bad_alloc&) {
+      d2h_err = cudaErrorMemoryAllocation;
+      return;
+    }
+    auto copy = [&](void* dst, const void* src, size_t bytes) {
+      if (d2h_err == cudaSuccess) d2h_err = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st2);
+    };
+    copy(t.coords.data(), T.coords, t.coords.size() * sizeof(int64_t));
+    copy(t.wall.data(), T.wall, n * sizeof(uint32_t));
+    copy(t.iolet.data(), T.iolet, n * sizeof(uint32_t));
+    copy(t.stype.data(), T.stype, n * sizeof(int32_t));
+    copy(t.iolet_id.data(), T.iolet_id, n * sizeof(int32_t));
+    copy(t.q.data(), T.q, t.q.size() * sizeof(float));
+    copy(t.normal.data(), T.normal, t.normal.size() * sizeof(float));
+    const cudaError_t e = cudaStreamSynchronize(st2);
+    if (d2h_err == cudaSuccess) d2h_err = e;
+  };
+  if (!layout) {
+    download();
+  } else {
+    std::thread th(download);
+    struct Join {
+      std::thread& th;
+      ~Join() {
+        if (th.joinable()) th.join();
+      }
+    } join{th};
+    DeviceTables dt;
+    dt.n = n;
+    for (int d = 0; d < 3; d++) dt.dims[d] = t.dims[d];
+    dt.coords = T.coords;
+    dt.wall = T.wall;
+    dt.iolet = T.iolet;
+    dt.stype = T.stype;
+    dt.iolet_id = T.iolet_id;
+    dt.q = T.q;
+    dt.normal = T.normal;
+    *layout = layout_on_device(dt, *params, st);
+    th.join();
+  }
+  if (d2h_err == cudaErrorMemoryAllocation) throw Error{HB_ERR_OOM, "host memory for the tables"};
+  cuda_check(d2h_err, "copy of the tables");
+  if (layout) finish_layout(*layout, t, *params, wall);
   tm.d2h_ms = ms_since(t4);
   if (timing) *timing = tm;
   return t;

@@ -40,6 +40,108 @@ __global__ void __launch_bounds__(256) k_bulk_m2(const StepArgs a, const MixArgs
   if (r1 >= 0) bulk_collide_m<S, K, MACRO>(a, m, s1, g1);
 }
 
+// Steady-state plain bulk sites of the FP16 shifted form (LBGK, TRT; no outputs),
+// SPT sites per thread (s, s + 256, ...), all gathered before any collides.
+// Each load is one address add: the run table row holds the plane offsets
+// i * np + run_off[i] (Solver::upload).  The collision runs on the stored
+// scale, G = kScale * g (kScale = kHalfScale for FP16, 1 for FP32), so a value
+// is converted but never rescaled on its way in or out: with D = sum G and
+// M = sum c G,
+//   geq_i = w_i (D - 3/2 |M|^2 / (kScale + D) + 9/2 (c_i.M)^2 / (kScale + D) + 3 c_i.M),
+// which is kScale times the unscaled equilibrium of kernels_mixed.cu's header.
+// Opposite directions share the even part of the equilibrium.  4M-site pipe,
+// FP16 bulk kernel 0.0963 -> 0.0850 ms (0.45 -> 0.51 of the measured copy
+// bandwidth), the whole FP16 step 33.1k -> 36.1k MLUPS.
+template <class S>
+struct Lp;
+template <>
+struct Lp<float> {
+  static constexpr float kScale = 1.0f;
+  static __device__ __forceinline__ float ld(const void* base, int64_t k) { return __ldg(static_cast<const float*>(base) + k); }
+  static __device__ __forceinline__ void st(void* base, int64_t k, float v) { static_cast<float*>(base)[k] = v; }
+};
+template <>
+struct Lp<__half> {
+  static constexpr float kScale = kHalfScale;
+  static __device__ __forceinline__ float ld(const void* base, int64_t k) {
+    return __half2float(__ldg(static_cast<const __half*>(base) + k));
+  }
+  static __device__ __forceinline__ void st(void* base, int64_t k, float v) { static_cast<__half*>(base)[k] = __float2half_rn(v); }
+};
+
+template <class S, int K>
+__device__ __forceinline__ void collide_scaled(const StepArgs& a, const MixArgs& m, int s, const float* G) {
+  float D = 0.0f, Mx = 0.0f, My = 0.0f, Mz = 0.0f;
+  bool bad = false;
+#pragma unroll
+  for (int i = 0; i < Q; i++) {
+    D += G[i];
+    Mx += (float)cx(i) * G[i];
+    My += (float)cy(i) * G[i];
+    Mz += (float)cz(i) * G[i];
+    bad |= !(wf(i) * Lp<S>::kScale + G[i] > 0.0f);
+  }
+  if (bad) atomicOr(a.status, kStatusUnstable);
+  const float inv = 1.0f / (Lp<S>::kScale + D);
+  const float nh = 4.5f * inv;
+  const float t1 = D - 1.5f * (Mx * Mx + My * My + Mz * Mz) * inv;
+  float neq[Q];
+  neq[0] = G[0] - wf(0) * t1;
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {  // (i, i + 1) are opposite directions
+    const float mde = (float)cx(i) * Mx + (float)cy(i) * My + (float)cz(i) * Mz;
+    const float even = wf(i) * (t1 + nh * mde * mde), odd = wf(i) * (3.0f * mde);
+    neq[i] = G[i] - (even + odd);
+    neq[i + 1] = G[i + 1] - (even - odd);
+  }
+  const float om = (float)a.omega;
+  if (K == kTRT) {
+    const float omm = (float)a.omega_minus;
+    Lp<S>::st(m.fout, s, G[0] + om * neq[0]);
+#pragma unroll
+    for (int i = 1; i < Q; i += 2) {
+      const float sym = 0.5f * om * (neq[i] + neq[i + 1]), asym = 0.5f * omm * (neq[i] - neq[i + 1]);
+      Lp<S>::st(m.fout, (int64_t)i * a.np + s, G[i] + sym + asym);
+      Lp<S>::st(m.fout, (int64_t)(i + 1) * a.np + s, G[i + 1] + sym - asym);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < Q; i++) Lp<S>::st(m.fout, (int64_t)i * a.np + s, G[i] + om * neq[i]);
+  }
+}
+
+template <class S, int K, int SPT>
+__global__ void __launch_bounds__(256) k_bulk_lp(const StepArgs a, const MixArgs m) {
+  const int s0 = blockIdx.x * (256 * SPT) + threadIdx.x;
+  int r[SPT];
+  float G[SPT][Q];
+#pragma unroll
+  for (int k = 0; k < SPT; k++) {
+    const int s = s0 + 256 * k;
+    r[k] = s < a.n ? __ldg(a.meta + s) : -1;
+  }
+#pragma unroll
+  for (int k = 0; k < SPT; k++) {
+    if (r[k] < 0) continue;
+    const int s = s0 + 256 * k;
+    const int4* o4 = reinterpret_cast<const int4*>(a.run_po) + 5 * r[k];
+    int po[20];
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const int4 v = __ldg(o4 + j);
+      po[4 * j] = v.x;
+      po[4 * j + 1] = v.y;
+      po[4 * j + 2] = v.z;
+      po[4 * j + 3] = v.w;
+    }
+#pragma unroll
+    for (int i = 0; i < Q; i++) G[k][i] = Lp<S>::ld(m.fin, (int64_t)s + po[i]);
+  }
+#pragma unroll
+  for (int k = 0; k < SPT; k++)
+    if (r[k] >= 0) collide_scaled<S, K>(a, m, s0 + 256 * k, G[k]);
+}
+
 // The boundary kernel is latency-bound: outside the LES kernel, GZS walls and
 // output steps it is held to 64 registers (eight blocks of 128 per SM; its own
 // allocation is 68-72), measured 30.3k -> 30.7k MLUPS for the FP32 step on the 4M pipe.
@@ -73,7 +175,12 @@ __global__ void k_from_aos_m(const double* aos, const int* st2ref, int n, int64_
 template <class S, int K, int WALL, bool GATHER, bool MACRO>
 void launch_m4(const StepArgs& a, const MixArgs& m, int which, cudaStream_t st) {
   if ((which & 1) && a.n > 0) {
-    if (GATHER && sizeof(S) == 2) k_bulk_m2<S, K, MACRO><<<(a.n + 511) / 512, 256, 0, st>>>(a, m);
+    // FP16 only: FP32 storage measured no faster with it (0.1060 against 0.1060 ms on the
+    // 4M pipe), and keeping FP32 on the general kernel's arithmetic keeps a sharded
+    // FP32 lattice bit-identical to the single lattice.
+    if (GATHER && !MACRO && (K == kLBGK || K == kTRT) && a.run_po && sizeof(S) == 2)
+      k_bulk_lp<S, (K == kTRT ? kTRT : kLBGK), 2><<<(a.n + 511) / 512, 256, 0, st>>>(a, m);
+    else if (GATHER && sizeof(S) == 2) k_bulk_m2<S, K, MACRO><<<(a.n + 511) / 512, 256, 0, st>>>(a, m);
     else k_bulk_m<S, K, GATHER, MACRO><<<(a.n + 255) / 256, 256, 0, st>>>(a, m);
   }
   if ((which & 2) && a.gen.G > 0) k_general_m<S, K, WALL, GATHER, MACRO><<<(a.gen.G + 127) / 128, 128, 0, st>>>(a, m);

@@ -313,25 +313,15 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
   L.g_iolet.resize(G);
   L.g_q.assign((size_t)18 * G, 0.0f);
   L.g_nrm.assign((size_t)3 * G, 0.0f);
-  for (int k = 0; k < 7; k++) L.kind_start[k] = 0;
 
-  // Iolet table index and the direction closest to each normal.
-  for (int k = 0; k < 32; k++) L.dir0[k] = 0;
-  for (int k = 0; k < p.n_inlets; k++) L.dir0[k] = closest_direction(p.inlets[k].normal);
-  for (int k = 0; k < p.n_outlets; k++) L.dir0[16 + k] = closest_direction(p.outlets[k].normal);
-  auto iolet_cfg = [&](int idx) -> const hb_iolet& { return idx < 16 ? p.inlets[idx] : p.outlets[idx - 16]; };
-
-  std::vector<std::vector<std::pair<int, int>>> cpl_sites(32);  // (ref index, g)
   for (int g = 0; g < G; g++) {
     const int s = gl[g];
     const int x = L.st2ref[s];
     L.meta[s] = -(g + 1);
     L.g_site[g] = s;
     L.g_run[g] = regular[s] ? run_of[s] : -1;
-    if (regular[s]) L.regular_general++;
     const int ct = t.collision_type(x);
     L.g_kind[g] = ct;
-    L.kind_start[ct + 1]++;
     // Only the links the site's streamer sends to a delegate carry a rule.
     L.g_wall[g] = (ct == 1 || ct >= 4) ? t.wall[x] : 0u;
     L.g_iolet[g] = ct >= 2 ? t.iolet[x] : 0u;
@@ -349,8 +339,35 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
       const int grp = t.stype[x] == 1 ? 0 : 1;
       const int cnt = grp == 0 ? p.n_inlets : p.n_outlets;
       if (id < 0 || id >= cnt) throw Error{HB_ERR_BAD_INDEX, "site refers to an iolet that the case does not define"};
-      const int idx = grp * 16 + id;
-      L.g_io[g] = idx;
+      L.g_io[g] = grp * 16 + id;
+    }
+  }
+  finish_layout(L, t, p, wall);
+  return L;
+}
+
+void finish_layout(Layout& L, const LatticeTables& t, const hb_params& p, int wall) {
+  const int n = L.n, G = L.G;
+  L.g_cpl.assign(G, -1);
+  L.regular_general = 0;
+  for (int k = 0; k < 7; k++) L.kind_start[k] = 0;
+  for (int g = 0; g < G; g++) {
+    if (L.g_run[g] >= 0) L.regular_general++;
+    L.kind_start[L.g_kind[g] + 1]++;
+  }
+  for (int k = 1; k < 7; k++) L.kind_start[k] += L.kind_start[k - 1];
+
+  // The direction closest to each iolet normal.
+  for (int k = 0; k < 32; k++) L.dir0[k] = 0;
+  for (int k = 0; k < p.n_inlets; k++) L.dir0[k] = closest_direction(p.inlets[k].normal);
+  for (int k = 0; k < p.n_outlets; k++) L.dir0[16 + k] = closest_direction(p.outlets[k].normal);
+  auto iolet_cfg = [&](int idx) -> const hb_iolet& { return idx < 16 ? p.inlets[idx] : p.outlets[idx - 16]; };
+
+  std::vector<std::vector<std::pair<int, int>>> cpl_sites(32);  // (ref index, g)
+  for (int g = 0; g < G; g++) {
+    const int x = L.st2ref[L.g_site[g]];
+    if (L.g_iolet[g]) {
+      const int idx = L.g_io[g];
       const int kind = iolet_cfg(idx).kind;
       if (kind == kWK3 || kind == kWK2) {
         bool couples = false;
@@ -360,23 +377,27 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
       }
     }
     if (wall == kGZS && L.g_wall[g]) {
+      // Slot d of a GZS wall link d with no rule behind it is pulled from the
+      // fluid neighbour the virtual node extrapolates from; the slot writers
+      // guarantee that neighbour exists, but it may be another shard's.
       for (int d = 1; d < Q; d++) {
         if (!((L.g_wall[g] >> (d - 1)) & 1u)) continue;
         const int i = inv(d);
         const bool bi = (L.g_iolet[g] >> (i - 1)) & 1u, bw = (L.g_wall[g] >> (i - 1)) & 1u;
-        const double q = t.q[(size_t)18 * x + d - 1];
-        if (q < 0.75 && !bi && !bw && src[(size_t)s * Q + d] < 0)
+        const float q = L.g_q[(size_t)(d - 1) * G + g];
+        const int from = L.g_src[(size_t)(d - 1) * G + g];  // the site itself where no bulk pull fills the slot
+        if (q < 0.75 && !bi && !bw && from == L.g_site[g])
           throw Error{HB_ERR_UNSUPPORTED, "GZS wall link without a fluid neighbour behind the site"};
-        if (q < 0.75 && !bi && !bw && src[(size_t)s * Q + d] >= n)
+        if (q < 0.75 && !bi && !bw && from >= n)
           throw Error{HB_ERR_UNSUPPORTED, "GZS wall link whose extrapolation neighbour lies in another shard"};
       }
     }
   }
-  for (int k = 1; k < 7; k++) L.kind_start[k] += L.kind_start[k - 1];
 
   // Windkessel coupling slots in reference order, and the centre site
   // (BoundaryValues::IsIOletCentreOnThisProc, src/lb/iolets/BoundaryValues.cc:103-121).
   int slot = 0;
+  L.couplings.clear();
   for (int idx = 0; idx < 32; idx++) {
     const int cnt = idx < 16 ? p.n_inlets : p.n_outlets;
     if ((idx % 16) >= cnt || (iolet_cfg(idx).kind != kWK3 && iolet_cfg(idx).kind != kWK2)) continue;
@@ -404,7 +425,51 @@ Layout build_layout(const LatticeTables& t, const hb_params& p, int wall) {
     L.couplings.push_back(c);
   }
   L.cpl_total = slot;
-  return L;
+}
+
+namespace {
+uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull) {
+  const unsigned char* b = static_cast<const unsigned char*>(data);
+  for (size_t k = 0; k < bytes; k++) {
+    h ^= b[k];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+template <class T>
+uint64_t fnv_vec(const std::vector<T>& v) {
+  const size_t count = v.size();
+  return fnv1a(v.data(), count * sizeof(T), fnv1a(&count, sizeof(count)));
+}
+}  // namespace
+
+void layout_digest(const Layout& L, uint64_t out[32]) {
+  for (int k = 0; k < 32; k++) out[k] = 0;
+  const int64_t sc[] = {L.n, L.n_halo, L.np, L.axis, L.runs, L.bulk_sites, L.G, L.regular_general, L.cpl_total};
+  uint64_t h = fnv1a(sc, sizeof(sc));
+  h = fnv1a(L.kind_start, sizeof(L.kind_start), h);
+  out[0] = fnv1a(L.dir0, sizeof(L.dir0), h);
+  out[1] = fnv_vec(L.st2ref);
+  out[2] = fnv_vec(L.ref2st);
+  out[3] = fnv_vec(L.meta);
+  out[4] = fnv_vec(L.run_off);
+  out[5] = fnv_vec(L.g_site);
+  out[6] = fnv_vec(L.g_run);
+  out[7] = fnv_vec(L.g_src);
+  out[8] = fnv_vec(L.g_io);
+  out[9] = fnv_vec(L.g_cpl);
+  out[10] = fnv_vec(L.g_xyz);
+  out[11] = fnv_vec(L.g_kind);
+  out[12] = fnv_vec(L.g_wall);
+  out[13] = fnv_vec(L.g_iolet);
+  out[14] = fnv_vec(L.g_q);
+  out[15] = fnv_vec(L.g_nrm);
+  uint64_t c = fnv1a(nullptr, 0);
+  for (const auto& cp : L.couplings) {
+    const int64_t v[] = {cp.iolet, cp.start, cp.count, cp.centre_ref, cp.centre_couples ? 1 : 0};
+    c = fnv1a(v, sizeof(v), c);
+  }
+  out[16] = c;
 }
 
 }  // namespace hb

@@ -43,6 +43,38 @@ struct Layout {
 // lattices whose streaming pattern the pull form cannot reproduce exactly.
 Layout build_layout(const LatticeTables& t, const hb_params& p, int wall);
 
+// The part of the layout that follows the general records (shared by the host
+// and the device builds): record bins, Windkessel couplings and centre sites,
+// the directions closest to the iolet normals, the GZS neighbour check.
+void finish_layout(Layout& L, const LatticeTables& t, const hb_params& p, int wall);
+
+// Lattice tables resident on the device (LatticeTables' fields, device pointers;
+// q and normal may be null).
+struct DeviceTables {
+  int64_t n = 0;
+  int64_t n_owned = -1;
+  int64_t dims[3] = {0, 0, 0};
+  const int64_t* coords = nullptr;
+  const uint32_t* wall = nullptr;
+  const uint32_t* iolet = nullptr;
+  const int32_t* stype = nullptr;
+  const int32_t* iolet_id = nullptr;
+  const float* q = nullptr;
+  const float* normal = nullptr;
+};
+
+// build_layout's passes up to the general records run on the GPU
+// (layout_device.cu) over tables already on the device, on `stream`; the
+// result is downloaded and equals build_layout's bit for bit once
+// finish_layout has run on it.  Neighbours come from the coordinates.
+Layout layout_on_device(const DeviceTables& d, const hb_params& p, void* stream);
+// The same from host tables (uploaded first).  Tables that carry their own
+// neighbour table are laid out on the host.
+Layout build_layout_on_device(const LatticeTables& t, const hb_params& p, int wall, int device);
+
+// FNV-1a digests of the layout's scalars and arrays (hb_geometry_layout_digest).
+void layout_digest(const Layout& L, uint64_t out[32]);
+
 // Direction closest to an iolet normal (SortDirectionsCloseToIOletNormal,
 // src/lb/streamers/NashZerothOrderPressureDelegate.h:95-116).
 int closest_direction(const double n[3]);

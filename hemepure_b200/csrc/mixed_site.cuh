@@ -214,41 +214,47 @@ __device__ __forceinline__ void gather_bulk_m(const StepArgs& a, const MixArgs& 
   for (int i = 1; i < Q; i++) g[i] = ldg_s<S>(m, (int64_t)i * a.np + (s + off[i]));
 }
 
+// Every slot's first value is one load (predicated between the ghost buffer and
+// the distributions, with no branch on the link masks): the ghost of an iolet
+// link, g*_d of the own site for a wall link, g*_i of the source site otherwise
+// (s + run offset for a record that follows its run, else its pull table).  The
+// BFL correction of wall links follows as a predicated step (as the FP64 kernel).
 template <class S, int WALL>
 __device__ __forceinline__ void gather_general_m(const StepArgs& a, const MixArgs& m, int gi, int s, float* g) {
   const GeneralDev& G = a.gen;
   const uint32_t wm = __ldg(G.wall + gi), im = __ldg(G.iolet + gi);
   const int run = __ldg(G.run + gi);
-  int off[20];
-  if (run >= 0) run_offsets(a, run, off);
+  int src[18];
+  if (run >= 0) {
+    int off[20];
+    run_offsets(a, run, off);
+#pragma unroll
+    for (int i = 1; i < Q; i++) src[i - 1] = s + off[i];
+  } else {
+#pragma unroll
+    for (int i = 1; i < Q; i++) src[i - 1] = __ldg(G.src + (int64_t)(i - 1) * G.G + gi);
+  }
   g[0] = ldg_s<S>(m, s);
 #pragma unroll
   for (int i = 1; i < Q; i++) {
     const int d = inv(i);
     const bool bw = (wm >> (d - 1)) & 1u, bi = (im >> (d - 1)) & 1u;
-    if (bi) {
-      g[i] = __ldg(m.gin + (int64_t)(d - 1) * G.G + gi);
-    } else if (bw) {
-      const float fd = ldg_s<S>(m, (int64_t)d * a.np + s);
-      if (WALL == kBFL) {
-        // The cut distance and both values are loaded before the rule is chosen.
-        const bool wi = (wm >> (i - 1)) & 1u;
-        if (wi) {
-          g[i] = fd;
-        } else {
-          const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
-          const float fi = ldg_s<S>(m, (int64_t)i * a.np + s);
-          g[i] = q < 0.5f ? fd : (fd + (2.0f * q - 1.0f) * fi) / (2.0f * q);
-        }
-      } else {
-        g[i] = fd;
-      }
-    } else {
-      const int src = run >= 0 ? s + off[i] : __ldg(G.src + (int64_t)(i - 1) * G.G + gi);
-      g[i] = ldg_s<S>(m, (int64_t)i * a.np + src);
-    }
+    const int64_t k = bw ? (int64_t)d * a.np + s : (int64_t)i * a.np + src[i - 1];
+    float v;
+    if (bi) v = __ldg(m.gin + (int64_t)(d - 1) * G.G + gi);
+    else v = ldg_s<S>(m, k);
+    g[i] = v;
   }
   if (WALL == kBFL && wm) {
+#pragma unroll
+    for (int i = 1; i < Q; i++) {
+      const int d = inv(i);
+      if (((wm >> (d - 1)) & 1u) && !((wm >> (i - 1)) & 1u) && !((im >> (d - 1)) & 1u)) {
+        const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
+        const float fi = ldg_s<S>(m, (int64_t)i * a.np + s);
+        if (!(q < 0.5f)) g[i] = (g[i] + (2.0f * q - 1.0f) * fi) / (2.0f * q);
+      }
+    }
 #pragma unroll
     for (int d = 1; d < Q; d++) {
       const int i = inv(d);

@@ -10,8 +10,10 @@
 //   EndIteration   swap the two buffers, time step + 1
 #include "solver.h"
 #include "shard.h"
+#include "extraction.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 
@@ -67,23 +69,27 @@ void upload_vec(DeviceBuffer& b, const std::vector<T>& v, int64_t& total) {
 
 }  // namespace
 
-Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& opt)
-    : t_(std::move(tables)), p_(params), opt_(opt) {
-  if (opt_.kernel < 0 || opt_.kernel > kTRTSL || opt_.wall < 0 || opt_.wall > 2) throw Error{HB_ERR_ARG, "unknown kernel or wall type"};
-  if (opt_.precision < HB_STORE_FP64 || opt_.precision > HB_STORE_FP16) throw Error{HB_ERR_ARG, "unknown storage precision"};
-  if (is_sponge(opt_.kernel) && opt_.wall == kGZS)
+void validate_case(const hb_params& p, const hb_options& o) {
+  if (o.kernel < 0 || o.kernel > kTRTSL || o.wall < 0 || o.wall > 2) throw Error{HB_ERR_ARG, "unknown kernel or wall type"};
+  if (o.precision < HB_STORE_FP64 || o.precision > HB_STORE_FP16) throw Error{HB_ERR_ARG, "unknown storage precision"};
+  if (is_sponge(o.kernel) && o.wall == kGZS)
     throw Error{HB_ERR_UNSUPPORTED, "GZS walls with a sponge-layer kernel: the virtual-node collision has no relaxation time"};
-  if ((opt_.kernel == kLBGKSL || opt_.kernel == kTRTSL) && opt_.precision != HB_STORE_FP64)
+  if ((o.kernel == kLBGKSL || o.kernel == kTRTSL) && o.precision != HB_STORE_FP64)
     throw Error{HB_ERR_UNSUPPORTED, "the LBGKSL and TRTSL kernels run with FP64 storage"};
-  if (!(p_.tau > 0.5)) throw Error{HB_ERR_ARG, "tau must exceed 1/2"};
-  for (int k = 0; k < p_.n_inlets + p_.n_outlets; k++) {
-    const hb_iolet& io = k < p_.n_inlets ? p_.inlets[k] : p_.outlets[k - p_.n_inlets];
+  if (!(p.tau > 0.5)) throw Error{HB_ERR_ARG, "tau must exceed 1/2"};
+  for (int k = 0; k < p.n_inlets + p.n_outlets; k++) {
+    const hb_iolet& io = k < p.n_inlets ? p.inlets[k] : p.outlets[k - p.n_inlets];
     if (io.kind < 0 || io.kind > kWomersley) throw Error{HB_ERR_ARG, "unknown iolet kind"};
     if ((io.kind == kFile || io.kind == kFileVelocity) && (!io.table || io.table_steps == 0))
       throw Error{HB_ERR_ARG, "a file iolet needs its table"};
     if (io.kind == kWomersley && !(io.period > 0.0 && io.radius > 0.0))
       throw Error{HB_ERR_ARG, "a Womersley iolet needs a positive period and radius"};
   }
+}
+
+Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& opt, Layout* layout)
+    : t_(std::move(tables)), p_(params), opt_(opt) {
+  validate_case(p_, opt_);
   // The file iolets' tables are the caller's only for the call: keep copies.
   for (int idx = 0; idx < 32; idx++) {
     const int cnt = idx < 16 ? p_.n_inlets : p_.n_outlets;
@@ -95,7 +101,8 @@ Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& 
   }
   if ((opt_.wall == kBFL || opt_.wall == kGZS) && t_.q.empty()) throw Error{HB_ERR_ARG, "BFL and GZS walls need wall distances"};
   check(cudaSetDevice(opt_.device), "cudaSetDevice");
-  L_ = build_layout(t_, p_, opt_.wall);
+  if (layout) L_ = std::move(*layout);
+  else L_ = build_layout(t_, p_, opt_.wall);
   t_step_ = p_.initial_step ? p_.initial_step : 1;
   omega_ = -1.0 / p_.tau;
   {
@@ -146,6 +153,13 @@ void Solver::upload() {
   }
   upload_vec(meta_, L_.meta, tot);
   upload_vec(run_off_, L_.run_off, tot);
+  if (opt_.precision == HB_STORE_FP16 && (int64_t)Q * np < ((int64_t)1 << 31)) {
+    // Plane offsets for the FP16 bulk kernel: one address add per load.
+    std::vector<int> po(L_.run_off.size(), 0);
+    for (size_t r = 0; r < po.size() / 20; r++)
+      for (int i = 0; i < Q; i++) po[r * 20 + i] = (int)((int64_t)i * np + L_.run_off[r * 20 + i]);
+    upload_vec(run_po_, po, tot);
+  }
   upload_vec(st2ref_, L_.st2ref, tot);
   upload_vec(g_site_, L_.g_site, tot);
   upload_vec(g_run_, L_.g_run, tot);
@@ -313,6 +327,7 @@ StepArgs Solver::args() const {
   a.n = L_.n;
   a.meta = meta_.as<int>();
   a.run_off = run_off_.as<int>();
+  a.run_po = run_po_.p ? run_po_.as<int>() : nullptr;
   a.gen.G = L_.G;
   a.gen.site = g_site_.as<int>();
   a.gen.run = g_run_.as<int>();
@@ -583,28 +598,122 @@ void Solver::materialise() {
   prev_valid_ = false;
 }
 
-bool Solver::get_previous_fs(double* f) {
+bool Solver::previous_aos_device(double* aos) {
   if (!prev_valid_) return false;
-  DeviceBuffer tmp;
-  tmp.alloc((size_t)L_.n * Q * sizeof(double));
   if (mixed()) {
-    to_aos(true, tmp.as<double>());
-    check(cudaMemcpyAsync(f, tmp.p, (size_t)L_.n * Q * sizeof(double), cudaMemcpyDeviceToHost, stream_), "f download");
-    check(cudaStreamSynchronize(stream_), "get_previous_fs");
+    to_aos(true, aos);
     return true;
   }
   StepArgs a = args();
   a.fin = f_[1 - cur_].as<double>();
   a.gin = ghost_[1 - cur_].as<double>();
   if (prev_direct_) {
-    launch_soa_to_aos_f64(a.fin, L_.np, st2ref_.as<int>(), L_.n, tmp.as<double>(), stream_);
+    launch_soa_to_aos_f64(a.fin, L_.np, st2ref_.as<int>(), L_.n, aos, stream_);
   } else {
-    launch_gather_aos_f64(a, opt_.wall, st2ref_.as<int>(), tmp.as<double>(), stream_);
+    launch_gather_aos_f64(a, opt_.wall, st2ref_.as<int>(), aos, stream_);
   }
   check(cudaGetLastError(), "previous-state gather");
+  return true;
+}
+
+bool Solver::get_previous_fs(double* f) {
+  DeviceBuffer tmp;
+  tmp.alloc((size_t)L_.n * Q * sizeof(double));
+  if (!previous_aos_device(tmp.as<double>())) return false;
   check(cudaMemcpyAsync(f, tmp.p, (size_t)L_.n * Q * sizeof(double), cudaMemcpyDeviceToHost, stream_), "f download");
   check(cudaStreamSynchronize(stream_), "get_previous_fs");
   return true;
+}
+
+Solver::Selection Solver::select(const hb_selector& sel, bool macro, const bool stress[6], bool distributions) {
+  const int n = L_.n;
+  const int64_t np = L_.np;
+  if (macro && (!macro_valid_ || !rho_.p))
+    throw Error{HB_ERR_ARG, "the last step did not fill the macroscopic caches (pass HB_STEP_MACRO)"};
+  for (int k = 0; k < 6; k++)
+    if (stress[k] && (!stress_valid_ || !pi_.p))
+      throw Error{HB_ERR_ARG, "the last step did not fill the stress caches (pass HB_STEP_MACRO | HB_STEP_STRESS)"};
+  if (!sel_coords_.p) {
+    std::vector<int32_t> c((size_t)3 * n);
+    std::vector<uint8_t> w(n), st(n);
+    for (int i = 0; i < n; i++) {
+      for (int d = 0; d < 3; d++) c[(size_t)3 * i + d] = (int32_t)t_.coords[(size_t)3 * i + d];
+      w[i] = t_.wall[i] != 0;
+      st[i] = (uint8_t)t_.stype[i];
+    }
+    std::vector<int> r2s(L_.ref2st.begin(), L_.ref2st.begin() + n);
+    int64_t tot = 0;
+    upload_vec(sel_coords_, c, tot);
+    upload_vec(sel_wall_, w, tot);
+    upload_vec(sel_stype_, st, tot);
+    upload_vec(ref2st_, r2s, tot);
+    dev_bytes_ += tot;
+  }
+  SelectArgs a{};
+  selector_state(sel, &a);  // the reference selectors' float state (extraction.cpp)
+  a.n = n;
+  a.coords = sel_coords_.as<int32_t>();
+  a.wall = sel_wall_.as<uint8_t>();
+  a.stype = sel_stype_.as<uint8_t>();
+  a.voxel = dx_;
+  for (int d = 0; d < 3; d++) a.origin[d] = origin_[d];
+  DeviceBuffer mask, counts, total, idx;
+  mask.alloc((size_t)std::max(1, n));
+  counts.alloc((size_t)std::max(1, select_blocks(n)) * sizeof(int));
+  total.alloc(sizeof(int));
+  idx.alloc((size_t)std::max(1, n) * sizeof(int));
+  launch_select(a, mask.as<uint8_t>(), counts.as<int>(), total.as<int>(), idx.as<int>(), stream_);
+  check(cudaGetLastError(), "selector launch");
+  int m = 0;
+  check(cudaMemcpyAsync(&m, total.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "selection count");
+  check(cudaStreamSynchronize(stream_), "selection");
+  Selection out;
+  out.idx.resize(m);
+  if (m > 0)
+    check(cudaMemcpyAsync(out.idx.data(), idx.p, (size_t)m * sizeof(int), cudaMemcpyDeviceToHost, stream_), "selection");
+  DeviceBuffer buf;
+  auto fetch = [&](const double* src, int64_t stride, int width, std::vector<double>& dst) {
+    dst.resize((size_t)m * width);
+    if (m == 0) return;
+    if (buf.bytes < (size_t)m * width * sizeof(double)) buf.alloc((size_t)m * 19 * sizeof(double));
+    launch_gather_selected(src, stride, width, idx.as<int>(), ref2st_.as<int>(), m, buf.as<double>(), stream_);
+    check(cudaGetLastError(), "selected gather");
+    check(cudaMemcpyAsync(dst.data(), buf.p, dst.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_), "selected download");
+    check(cudaStreamSynchronize(stream_), "selected download");
+  };
+  if (macro) {
+    fetch(rho_.as<double>(), np, 1, out.rho);
+    fetch(u_.as<double>(), np, 3, out.u);
+    fetch(wss_.as<double>(), np, 1, out.wss);
+  }
+  for (int k = 0; k < 6; k++) {
+    if (!stress[k]) continue;
+    if (!stress_out_.p) {
+      stress_out_.alloc((size_t)6 * np * sizeof(double));
+      dev_bytes_ += (int64_t)stress_out_.bytes;
+    }
+    StepArgs sa = args();
+    sa.pi = pi_.as<double>();
+    launch_stress_field(sa, k, stress_out_.as<double>(), stream_);
+    check(cudaGetLastError(), "stress field launch");
+    fetch(stress_out_.as<double>(), np, stress_len(k), out.stress[k]);
+  }
+  if (distributions) {
+    DeviceBuffer aos;
+    aos.alloc((size_t)std::max(1, n) * Q * sizeof(double));
+    if (!previous_aos_device(aos.as<double>()))
+      throw Error{HB_ERR_ARG, "the distributions of the last step are no longer held"};
+    out.fd.resize((size_t)m * Q);
+    if (m > 0) {
+      buf.alloc((size_t)m * Q * sizeof(double));
+      launch_gather_rows(aos.as<double>(), Q, idx.as<int>(), m, buf.as<double>(), stream_);
+      check(cudaGetLastError(), "selected rows");
+      check(cudaMemcpyAsync(out.fd.data(), buf.p, out.fd.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+            "selected download");
+    }
+  }
+  check(cudaStreamSynchronize(stream_), "selection");
+  return out;
 }
 
 void Solver::set_units(double dt, double dx, const double origin[3]) {
@@ -737,6 +846,92 @@ void Solver::moment_sums(double out[4]) {
   check(cudaGetLastError(), "moment sums launch");
   check(cudaMemcpyAsync(out, sum_out_.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, stream_), "sums download");
   check(cudaStreamSynchronize(stream_), "moment_sums");
+}
+
+// File layout of write_state (host byte order, little-endian on these hosts):
+// char[8] "HBSTATE1"; int64 n, uint64 time step, int32 Windkessel iolets W,
+// int32 coupling slots C; int64 coords[n*3] (reference order, to check the
+// lattice on restore); double f[n*19] (AoS, reference order: the pre-collision
+// distributions of the next step); W records of double density, density_new,
+// flow, flow_old and int64 sites summed at the previous step; double cpl[C].
+void Solver::write_state(const std::string& path) {
+  if (mixed()) throw Error{HB_ERR_UNSUPPORTED, "the FP64 state file holds FP64 storage only"};
+  const int64_t n = L_.n;
+  std::vector<double> f((size_t)n * Q);
+  get_fs(f.data());
+  std::vector<WK3Dev> wk(nwk3_);
+  if (nwk3_)
+    check(cudaMemcpyAsync(wk.data(), wk3_.p, wk.size() * sizeof(WK3Dev), cudaMemcpyDeviceToHost, stream_), "state");
+  const int32_t ncpl = L_.cpl_total;
+  std::vector<double> cpl(std::max(1, ncpl));
+  check(cudaMemcpyAsync(cpl.data(), cpl_buf_.p, cpl.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_), "state");
+  check(cudaStreamSynchronize(stream_), "state");
+  FILE* fh = std::fopen(path.c_str(), "wb");
+  if (!fh) throw Error{HB_ERR_IO, "cannot write " + path};
+  bool ok = std::fwrite("HBSTATE1", 1, 8, fh) == 8;
+  const uint64_t t = t_step_;
+  const int32_t w = nwk3_;
+  ok = ok && std::fwrite(&n, 8, 1, fh) == 1 && std::fwrite(&t, 8, 1, fh) == 1 && std::fwrite(&w, 4, 1, fh) == 1 &&
+       std::fwrite(&ncpl, 4, 1, fh) == 1;
+  ok = ok && std::fwrite(t_.coords.data(), 8, (size_t)3 * n, fh) == (size_t)3 * n;
+  ok = ok && std::fwrite(f.data(), 8, f.size(), fh) == f.size();
+  for (const WK3Dev& x : wk) {
+    const double v[4] = {x.density, x.density_new, x.flow, x.flow_old};
+    const int64_t c = x.count_prev;
+    ok = ok && std::fwrite(v, 8, 4, fh) == 4 && std::fwrite(&c, 8, 1, fh) == 1;
+  }
+  ok = ok && std::fwrite(cpl.data(), 8, (size_t)ncpl, fh) == (size_t)ncpl;
+  ok = (std::fclose(fh) == 0) && ok;
+  if (!ok) throw Error{HB_ERR_IO, "cannot write " + path};
+}
+
+void Solver::read_state(const std::string& path) {
+  if (mixed()) throw Error{HB_ERR_UNSUPPORTED, "the FP64 state file holds FP64 storage only"};
+  FILE* fh = std::fopen(path.c_str(), "rb");
+  if (!fh) throw Error{HB_ERR_IO, "cannot open " + path};
+  struct Closer {
+    FILE* f;
+    ~Closer() { std::fclose(f); }
+  } closer{fh};
+  char magic[8];
+  int64_t n = 0;
+  uint64_t t = 0;
+  int32_t w = 0, ncpl = 0;
+  if (std::fread(magic, 1, 8, fh) != 8 || std::memcmp(magic, "HBSTATE1", 8) != 0 || std::fread(&n, 8, 1, fh) != 1 ||
+      std::fread(&t, 8, 1, fh) != 1 || std::fread(&w, 4, 1, fh) != 1 || std::fread(&ncpl, 4, 1, fh) != 1)
+    throw Error{HB_ERR_FORMAT, path + ": not a state file"};
+  if (n != L_.n || w != nwk3_ || ncpl != L_.cpl_total)
+    throw Error{HB_ERR_FORMAT, path + ": the state file belongs to another lattice or case"};
+  std::vector<int64_t> coords((size_t)3 * n);
+  std::vector<double> f((size_t)n * Q);
+  if (std::fread(coords.data(), 8, coords.size(), fh) != coords.size() || std::fread(f.data(), 8, f.size(), fh) != f.size())
+    throw Error{HB_ERR_FORMAT, path + ": truncated state file"};
+  if (std::memcmp(coords.data(), t_.coords.data(), coords.size() * 8) != 0)
+    throw Error{HB_ERR_FORMAT, path + ": the state file's sites are not this lattice's, in this order"};
+  std::vector<WK3Dev> wk(nwk3_);
+  if (nwk3_)
+    check(cudaMemcpyAsync(wk.data(), wk3_.p, wk.size() * sizeof(WK3Dev), cudaMemcpyDeviceToHost, stream_), "state");
+  check(cudaStreamSynchronize(stream_), "state");
+  for (WK3Dev& x : wk) {
+    double v[4];
+    int64_t c = 0;
+    if (std::fread(v, 8, 4, fh) != 4 || std::fread(&c, 8, 1, fh) != 1) throw Error{HB_ERR_FORMAT, path + ": truncated state file"};
+    x.density = v[0];
+    x.density_new = v[1];
+    x.flow = v[2];
+    x.flow_old = v[3];
+    x.count_prev = (int)c;
+  }
+  std::vector<double> cpl(std::max(1, ncpl), 0.0);
+  if (std::fread(cpl.data(), 8, (size_t)ncpl, fh) != (size_t)ncpl) throw Error{HB_ERR_FORMAT, path + ": truncated state file"};
+  set_fs(f.data());
+  if (nwk3_)
+    check(cudaMemcpyAsync(wk3_.p, wk.data(), wk.size() * sizeof(WK3Dev), cudaMemcpyHostToDevice, stream_), "state");
+  check(cudaMemcpyAsync(cpl_buf_.p, cpl.data(), cpl.size() * sizeof(double), cudaMemcpyHostToDevice, stream_), "state");
+  check(cudaStreamSynchronize(stream_), "state");
+  t_step_ = t;
+  rows_valid_ = false;
+  macro_valid_ = stress_valid_ = false;
 }
 
 void Solver::get_wk3(int group, int index, double st[4]) {

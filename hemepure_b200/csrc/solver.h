@@ -26,9 +26,15 @@ struct DeviceBuffer {
   T* as() const { return static_cast<T*>(p); }
 };
 
+// The checks of a case's parameters and options that need no lattice (the
+// solver's constructor runs them first); throws hb::Error.
+void validate_case(const hb_params& p, const hb_options& o);
+
 class Solver {
  public:
-  Solver(LatticeTables tables, const hb_params& params, const hb_options& opt);
+  // `layout`, when given, is the storage layout already built for these tables,
+  // parameters and wall rule (moved from); otherwise it is built here.
+  Solver(LatticeTables tables, const hb_params& params, const hb_options& opt, Layout* layout = nullptr);
   ~Solver();
 
   // lb::LBM phases.
@@ -76,6 +82,23 @@ class Solver {
   bool get_previous_fs(double* f);
   void set_time_step(uint64_t t) { t_step_ = t; }
 
+  // Exact FP64 restart: the distributions entering the next step, the time
+  // step, and the Windkessel state with the coupling contributions the next
+  // step's flow sum reads (FP64 storage only).
+  void write_state(const std::string& path);
+  void read_state(const std::string& path);
+
+  // The sites a geometry selector takes (reference order) and the requested
+  // data of those sites only, selected and gathered on the device so that only
+  // they cross to the host: density, velocity, WSS of the last output step
+  // [m], [m*3], [m]; stress caches [m*k]; pre-collision f of the last step [m*19].
+  struct Selection {
+    std::vector<int> idx;
+    std::vector<double> rho, u, wss, fd;
+    std::vector<double> stress[6];
+  };
+  Selection select(const hb_selector& sel, bool macro, const bool stress[6], bool distributions);
+
   // Sharded form (tables cut by cut_shard): the halo lists of the slab
   // [lo, hi) along `axis`; then, after every step, pack the values the two
   // neighbours pull and, before the next, unpack theirs.  Both run on the
@@ -117,7 +140,7 @@ class Solver {
   DeviceBuffer ghost_[2];         // iolet ghost values, paired with f_
   int cur_ = 0;
   bool direct_ = true;            // f_[cur_] holds pre-collision f (else post-collision f*)
-  DeviceBuffer meta_, run_off_, st2ref_;
+  DeviceBuffer meta_, run_off_, run_po_, st2ref_;
   DeviceBuffer g_run_;
   DeviceBuffer g_site_, g_wall_, g_iolet_, g_src_, g_q_, g_nrm_, g_io_, g_cpl_, g_xyz_;
   DeviceBuffer g_wom_, wom_amp_;     // Womersley link factors (allocated only with such an iolet)
@@ -150,6 +173,10 @@ class Solver {
   bool prev_direct_ = false;
   double dt_ = 1.0, dx_ = 1.0;
   double origin_[3] = {0, 0, 0};
+  // Device copies of the tables a selector reads (made at the first selection).
+  DeviceBuffer sel_coords_, sel_wall_, sel_stype_, ref2st_;
+  // Pre-collision f of the last completed step, AoS in reference order, into a device buffer.
+  bool previous_aos_device(double* aos);
   // Sharded form.
   bool shard_ = false;
   int64_t send_n_[2] = {0, 0}, recv_n_[2] = {0, 0};

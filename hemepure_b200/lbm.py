@@ -42,15 +42,15 @@ EXPORTS = [
     "hb_step", "hb_site_count", "hb_time_step", "hb_get_params", "hb_get_fs", "hb_set_fs",
     "hb_get_macro", "hb_get_stress", "hb_set_iolet_densities", "hb_get_wk3", "hb_get_tables", "hb_write_xtr", "hb_read_checkpoint",
     "hb_last_step_timing", "hb_device_bytes", "hb_read_case", "hb_geometry_open", "hb_geometry_site_count",
-    "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_close", "hb_profile_steps",
+    "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_layout_digest", "hb_geometry_close", "hb_profile_steps",
     "hb_set_time_step", "hb_moment_sums", "hb_moment_sums_noalloc",
     "hb_batch_bytes", "hb_batch_create", "hb_batch_destroy", "hb_batch_add_xml", "hb_batch_add", "hb_batch_remove",
     "hb_batch_run", "hb_batch_get_macro", "hb_batch_member_info", "hb_batch_set_tuning", "hb_batch_set_step_form",
     "hb_batch_stats",
-    "hb_batch_prepare_xml", "hb_batch_prep_sites", "hb_batch_add_prepared", "hb_batch_prep_free",
+    "hb_batch_prepare_xml", "hb_batch_prepare_xml_device", "hb_batch_prep_sites", "hb_batch_add_prepared", "hb_batch_prep_free",
     "hb_write_xtr_selected", "hb_geometry_select", "hb_read_case_iolet_table", "hb_iolet_velocity",
     "hb_shard_plan", "hb_create_shard_from_xml", "hb_shard_halo_sizes", "hb_shard_pack", "hb_shard_unpack",
-    "hb_shard_site_ids", "hb_shard_describe",
+    "hb_shard_site_ids", "hb_shard_describe", "hb_write_state", "hb_read_state",
     "hb_geometry_open_device", "hb_geometry_read_timing",
 ]
 
@@ -162,6 +162,7 @@ def library() -> C.CDLL:
     L.hb_geometry_site_count.argtypes = [P, P, P]
     L.hb_geometry_tables.argtypes = [P] + [P] * 9
     L.hb_geometry_layout.argtypes = [P, P, I, P]
+    L.hb_geometry_layout_digest.argtypes = [P, P, I, I, P]
     L.hb_geometry_close.argtypes = [P]
     L.hb_profile_steps.argtypes = [P, I64, P]
     L.hb_set_time_step.argtypes = [P, U64]
@@ -180,9 +181,12 @@ def library() -> C.CDLL:
     L.hb_batch_set_step_form.argtypes = [P, I]
     L.hb_batch_stats.argtypes = [P, P, P, P]
     L.hb_batch_prepare_xml.argtypes = [C.c_char_p, I, I, U64, C.POINTER(P)]
+    L.hb_batch_prepare_xml_device.argtypes = [C.c_char_p, I, I, U64, I, C.POINTER(P)]
     L.hb_batch_prep_sites.argtypes = [P, P]
     L.hb_batch_add_prepared.argtypes = [P, P, P]
     L.hb_batch_prep_free.argtypes = [P]
+    L.hb_write_state.argtypes = [P, C.c_char_p]
+    L.hb_read_state.argtypes = [P, C.c_char_p]
     L.hb_shard_plan.argtypes = [C.c_char_p, I, I, P, P]
     L.hb_create_shard_from_xml.argtypes = [C.c_char_p, P, P, C.POINTER(P)]
     L.hb_shard_halo_sizes.argtypes = [P, P, P]
@@ -426,6 +430,14 @@ class LBM:
         library().hb_last_step_timing(self._h, C.byref(ms), C.byref(n))
         return float(ms.value), int(n.value)
 
+    def WriteState(self, path) -> None:
+        """Exact FP64 restart file (hb_write_state)."""
+        self._check(library().hb_write_state(self._h, os.fspath(path).encode()))
+
+    def ReadState(self, path) -> None:
+        """Restore a run from hb_write_state's file: it continues bit for bit."""
+        self._check(library().hb_read_state(self._h, os.fspath(path).encode()))
+
     # -- sharded form -------------------------------------------------------------------
     def shard_halo_sizes(self):
         """Stored elements (send lower, send upper, receive lower, receive upper)
@@ -564,6 +576,15 @@ class Geometry:
             raise HemeLBError(rc, last_create_error())
         return {"axis": int(st[0]), "runs": int(st[1]), "bulk_sites": int(st[2]), "general_sites": int(st[3])}
 
+    def layout_digest(self, params: Params, wall: str = "SBB", device: int = -1) -> np.ndarray:
+        """Digests of every array of the storage layout, built on the host
+        (device < 0) or on that GPU; the two builds agree bit for bit."""
+        out = np.zeros(32, np.uint64)
+        rc = library().hb_geometry_layout_digest(self._g, C.byref(params), WALLS[wall], int(device), _p(out))
+        if rc != HB_OK:
+            raise HemeLBError(rc, last_create_error())
+        return out
+
     def close(self):
         if getattr(self, "_g", None) and self._g.value:
             library().hb_geometry_close(self._g)
@@ -579,12 +600,19 @@ class Geometry:
 class PreparedLattice:
     """A case parsed, its geometry read and its storage layout built on the
     host, ready for Batch.add_prepared.  Preparation needs no device and releases
-    the interpreter lock, so it runs on worker threads while blocks step."""
+    the interpreter lock, so it runs on worker threads while blocks step.  With
+    `device`, the geometry is decoded and laid out on that GPU instead (same
+    result; it synchronises the device)."""
 
-    def __init__(self, xml_path: str, kernel: str = "LBGK", wall: str = "SBB", steps: int = 1000):
+    def __init__(self, xml_path: str, kernel: str = "LBGK", wall: str = "SBB", steps: int = 1000,
+                 device: Optional[int] = None):
         self._h = C.c_void_p()
-        rc = library().hb_batch_prepare_xml(os.fspath(xml_path).encode(), KERNELS[kernel], WALLS[wall], int(steps),
-                                            C.byref(self._h))
+        if device is None:
+            rc = library().hb_batch_prepare_xml(os.fspath(xml_path).encode(), KERNELS[kernel], WALLS[wall], int(steps),
+                                                C.byref(self._h))
+        else:
+            rc = library().hb_batch_prepare_xml_device(os.fspath(xml_path).encode(), KERNELS[kernel], WALLS[wall],
+                                                       int(steps), int(device), C.byref(self._h))
         if rc != HB_OK:
             raise HemeLBError(rc, last_create_error())
         n = C.c_int64()

@@ -38,6 +38,7 @@ class Request:
     # filled by the server
     admitted: Optional[float] = None
     finished: Optional[float] = None
+    steps_done: int = 0      # time steps the lattice made (its step count unless it went unstable)
     result: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
     status: int = 0          # status bits of the run (1 unstable, 2 iolet radius), or a negative error code
     error: str = ""
@@ -274,17 +275,18 @@ class Server:
                     if pending and not self.queue:
                         time.sleep(max(0.0, min(0.05, pending[0].arrival - (clock() - t0))))
                     continue
-                active = self.batch.stats()[1]
                 done = self.batch.run(self.block_steps)
                 ms = self.batch.stats()[0]
                 self.device_ms += ms
                 self.blocks += 1
-                self.site_updates += active * self.block_steps
                 now = clock() - t0
                 for slot in done:
                     r = self.running.pop(slot)
                     n, t, st = self.batch.info(slot)
                     r.status = st
+                    # Work up to the member's own last step, not to the block's end.
+                    r.steps_done = r.steps if st == 0 else max(0, min(r.steps, int(t) - 1))
+                    self.site_updates += r.sites * r.steps_done
                     if st == 0:          # an unstable lattice is handed back early, without fields
                         res = self.batch.macro(slot)
                         if keep_results:
@@ -296,21 +298,60 @@ class Server:
             self.pool.shutdown(wait=True)
         self.wall_s = clock() - t0
 
+    def close(self) -> None:
+        """Release the batch's device memory."""
+        self.batch.close()
+
     def report(self) -> Dict[str, float]:
-        """Latency percentiles over all requests; aggregate MLUPS counts the site
-        updates of the requests that completed (a request whose lattice went
-        unstable is retired at once and counted as failed, not as work)."""
+        """Latency percentiles over all requests and over the first and second
+        halves of the stream (by arrival: a stationary queue gives the two halves
+        the same latencies); aggregate MLUPS counts the site updates of the
+        requests that completed (a request whose lattice went unstable is
+        retired at once and counted as failed, not as work); device-busy MLUPS
+        counts every member's steps up to its own end over the device time."""
         lat = np.array([r.latency for r in self.completed])
         work = sum(r.sites * r.steps for r in self.completed if not r.status)
         failed = [r for r in self.completed if r.status]
+        by_arrival = sorted(self.completed, key=lambda r: r.arrival)
+        half = len(by_arrival) // 2
+        halves = {}
+        for name, part in (("first_half", by_arrival[:half]), ("second_half", by_arrival[half:])):
+            if part:
+                lh = np.array([r.latency for r in part])
+                halves[name] = {"requests": len(part), "p50_latency_s": float(np.percentile(lh, 50)),
+                                "p99_latency_s": float(np.percentile(lh, 99))}
         return {"requests": len(self.completed), "p50_latency_s": float(np.percentile(lat, 50)),
                 "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
+                "halves": halves,
                 "aggregate_MLUPS": work / self.wall_s / 1e6, "wall_s": self.wall_s,
                 "device_busy_MLUPS": self.site_updates / (self.device_ms * 1e-3) / 1e6 if self.device_ms else 0.0,
                 "device_busy_fraction": self.device_ms * 1e-3 / self.wall_s if self.wall_s else 0.0,
                 "blocks": self.blocks, "site_capacity": self.site_capacity, "failed": len(failed),
                 "failed_requests": [{"rid": r.rid, "status": r.status, "shape": r.shape, "sites": r.sites}
                                     for r in failed]}
+
+
+def sustained_rate(requests: Sequence[Request], budget_bytes: int, tuning: Optional[Tuning] = None, device: int = 0,
+                   block_steps: int = 200) -> Dict[str, float]:
+    """Closed-loop saturation pass: the given requests (the head of the stream)
+    all arrive at once and the server runs them to completion under the same
+    budget, block length and tuning as the open-loop run.  Their work over the
+    wall time is the throughput the server sustains on this mix with admissions,
+    retirements and block boundaries included, the rate an arrival process must
+    stay below for the queue to be stationary."""
+    import copy
+    reqs = [copy.copy(r) for r in requests]
+    for r in reqs:
+        r.arrival = 0.0
+        r.admitted = r.finished = None
+        r.result = None
+        r.status, r.steps_done, r.error = 0, 0, ""
+    srv = Server(budget_bytes, device=device, tuning=tuning, block_steps=block_steps)
+    srv.run(reqs)
+    rep = srv.report()
+    srv.close()
+    return {"MLUPS": rep["aggregate_MLUPS"], "requests": len(reqs), "wall_s": rep["wall_s"],
+            "device_busy_MLUPS": rep["device_busy_MLUPS"]}
 
 
 def solve_sequential_fp64(requests: Sequence[Request], device: int = 0) -> Dict[str, float]:
@@ -363,3 +404,73 @@ def _main(argv=None) -> None:
 
 if __name__ == "__main__":
     _main()
+
+
+# ---------------------------------------------------------------------------
+# Several GPUs: independent servers, one per device
+# ---------------------------------------------------------------------------
+
+def assign_least_work(requests: Sequence[Request], n_devices: int) -> List[List[Request]]:
+    """Each request, in arrival order, to the device with the least work (sites x
+    steps) assigned so far; ties to the lower device index.  Independent
+    lattices need no exchange, so the devices serve their shares apart."""
+    shares: List[List[Request]] = [[] for _ in range(n_devices)]
+    load = [0] * n_devices
+    for r in sorted(requests, key=lambda q: (q.arrival, q.rid)):
+        d = min(range(n_devices), key=lambda k: (load[k], k))
+        shares[d].append(r)
+        load[d] += r.sites * r.steps
+    return shares
+
+
+def _serve_share(args):
+    """One device's share, in its own process: its own CUDA context and server."""
+    (device, share, budget_bytes, tuning, block_steps, factory) = args
+    make = factory or (lambda dev: Server(budget_bytes, device=dev, tuning=tuning, block_steps=block_steps))
+    srv = make(device)
+    srv.run(share)
+    out = [(r.rid, r.admitted, r.finished, r.status, r.steps_done) for r in srv.completed]
+    rep = srv.report()
+    if hasattr(srv, "close"):
+        srv.close()
+    return device, out, rep
+
+
+class Dispatcher:
+    """Spreads a request stream over the GPUs of one node as replicas: one
+    `Server` per device, each in its own process (one CUDA context per GPU, as
+    one process per GPU), each request assigned on arrival order to the device
+    with the least assigned work.  All devices start at the same time, so the
+    arrival times keep their meaning; latencies and work come back per request.
+    `server_factory(device)` builds a server (a stand-in without a GPU in tests)."""
+
+    def __init__(self, devices: Sequence[int], budget_bytes: int, tuning: Optional[Tuning] = None,
+                 block_steps: int = 200, server_factory=None):
+        self.devices = list(devices)
+        self.budget_bytes, self.tuning, self.block_steps = budget_bytes, tuning, block_steps
+        self.factory = server_factory
+
+    def run(self, requests: Sequence[Request]) -> Dict[str, object]:
+        import multiprocessing as mp
+        shares = assign_least_work(requests, len(self.devices))
+        jobs = [(dev, share, self.budget_bytes, self.tuning, self.block_steps, self.factory)
+                for dev, share in zip(self.devices, shares)]
+        by_rid = {r.rid: r for r in requests}
+        t0 = time.perf_counter()
+        with ProcessPoolExecutor(max_workers=len(jobs), mp_context=mp.get_context("spawn")) as ex:
+            results = list(ex.map(_serve_share, jobs))
+        wall = time.perf_counter() - t0
+        per_device = {}
+        for dev, out, rep in results:
+            per_device[dev] = rep
+            for rid, admitted, finished, status, steps_done in out:
+                r = by_rid[rid]
+                r.admitted, r.finished, r.status, r.steps_done = admitted, finished, status, steps_done
+        done = [r for r in requests if r.finished is not None]
+        lat = np.array([r.latency for r in done]) if done else np.zeros(1)
+        work = sum(r.sites * r.steps for r in done if not r.status)
+        span = max((rep["wall_s"] for rep in per_device.values()), default=wall)
+        return {"devices": len(self.devices), "requests": len(done), "p50_latency_s": float(np.percentile(lat, 50)),
+                "p99_latency_s": float(np.percentile(lat, 99)), "aggregate_MLUPS": work / span / 1e6 if span else 0.0,
+                "wall_s": span, "failed": sum(1 for r in done if r.status),
+                "assigned_work": [sum(r.sites * r.steps for r in s) for s in shares], "per_device": per_device}

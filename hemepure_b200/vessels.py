@@ -627,11 +627,14 @@ def write_case_xml(path: str, gmy_name: str, vessel: Vessel, units: CaseUnits, s
 # ---------------------------------------------------------------------------
 
 def make_case(name: str, out_dir: str, steps: Optional[int] = None, scale: float = 1.0,
-              seed: int = 1234) -> Tuple[str, str, GeometryInfo]:
+              seed: int = 1234, tau: Optional[float] = None, inflow_scale: float = 1.0) -> Tuple[str, str, GeometryInfo]:
     """Write one of the named workloads into `out_dir`; returns (xml, gmy, info).
 
     `scale` < 1 shrinks radii and lengths (for fast parity tests) while keeping
-    the physics choices (kernel, walls, iolets)."""
+    the physics choices (kernel, walls, iolets).  `tau` replaces the workload's
+    relaxation time (the bifurcation's tau+) and `inflow_scale` multiplies the
+    stenosis's inlet speeds: variants of a workload that stay stable for its
+    full step count where the stated parameters do not."""
     os.makedirs(out_dir, exist_ok=True)
     rng = np.random.default_rng(seed)
     gmy = os.path.join(out_dir, f"{name}.gmy")
@@ -665,7 +668,7 @@ def make_case(name: str, out_dir: str, steps: Optional[int] = None, scale: float
         # Y-bifurcation, TRT (magic 3/16, tau+=0.52), GZS walls, cosine pressure
         # inlet (mean 1, amplitude 1e-3, period 4000), two WK3 outlets.
         v = YBifurcation(sc(32), sc(400, 8), sc(25), sc(400, 8), 35.0)
-        u = CaseUnits(tau=0.52)
+        u = CaseUnits(tau=tau or 0.52)
         # Windkessel sizing.  The reference integrates the absolute lattice pressure
         # (InOutLetWK3.cc:72-91), so the total resistance must carry the outlet at
         # p = cs^2 rho with rho ~ 1 for the Poiseuille flow the branches admit; the
@@ -690,12 +693,12 @@ def make_case(name: str, out_dir: str, steps: Optional[int] = None, scale: float
         # reference's InOutLetFileVelocity (a parabolic profile whose peak speed
         # is read from a file of time/speed pairs, one every 50 steps here).
         v = Stenosis(sc(48), sc(1200, 8), sc(24), max(4.0, 96 * scale))
-        u = CaseUnits(tau=0.502)
+        u = CaseUnits(tau=tau or 0.502)
         n_steps = steps or 20000
         table = os.path.join(out_dir, "stenosis_inflow.txt")
         with open(table, "w") as fh:
             for k in range(0, n_steps + 101, 50):
-                peak = 0.05 * (1.0 + 0.5 * math.sin(2.0 * math.pi * k / 10000.0))
+                peak = inflow_scale * 0.05 * (1.0 + 0.5 * math.sin(2.0 * math.pi * k / 10000.0))
                 fh.write(f"{k * u.dt!r} {u.speed_to_phys(peak)!r}\n")
         write_case_xml(xml, os.path.basename(gmy), v, u, n_steps,
                        [FileVelocityBC(os.path.basename(table))], [PressureBC(1.0)],

@@ -180,6 +180,19 @@ int hb_end_iteration(hb_handle* h);
  * A shard (below) advances one step per call. */
 int hb_step(hb_handle* h, int64_t n_steps, uint32_t flags);
 
+/* ---- exact restart in FP64 ------------------------------------------------------
+ * No counterpart in the reference, whose checkpoint is the float32
+ * "distributions" field of an .xtr file (LocalDistributionInput,
+ * src/extraction/LocalDistributionInput.cc:48-298; hb_read_checkpoint reads it),
+ * so a restart from it is not the run that would have continued.  This state
+ * file holds the distributions entering the next step in FP64, the time step,
+ * and each Windkessel iolet's state with the coupling contributions its next
+ * flow sum reads: a run restored from it continues bit for bit.  FP64 storage
+ * only (HB_ERR_UNSUPPORTED otherwise); the restore checks that the file's sites
+ * are the handle's, in the same order (HB_ERR_FORMAT otherwise). */
+int hb_write_state(hb_handle* h, const char* path);
+int hb_read_state(hb_handle* h, const char* path);
+
 /* ---- one lattice over several GPUs: slabs with a halo exchange --------------
  * The reference decomposes a lattice over MPI ranks
  * (src/geometry/decomposition/BasicDecomposition.cc:42-64, refined by
@@ -352,6 +365,12 @@ int hb_batch_remove(hb_batch* b, int slot);
  * object with hb_batch_prep_free either way. */
 typedef struct hb_batch_prep hb_batch_prep;
 int hb_batch_prepare_xml(const char* xml_path, int kernel, int wall, uint64_t steps, hb_batch_prep** out);
+/* The same with the site records decoded and the storage layout built on
+ * `device` (the result is identical).  Its device allocations and frees
+ * synchronise that device, so a server preparing while a batch steps on the
+ * same device keeps to hb_batch_prepare_xml. */
+int hb_batch_prepare_xml_device(const char* xml_path, int kernel, int wall, uint64_t steps, int device,
+                                hb_batch_prep** out);
 int hb_batch_prep_sites(const hb_batch_prep* prep, int64_t* sites);
 int hb_batch_add_prepared(hb_batch* b, hb_batch_prep* prep, int* slot);
 int hb_batch_prep_free(hb_batch_prep* prep);
@@ -414,6 +433,14 @@ int hb_geometry_tables(const hb_geometry* g, int64_t* neighbours, uint32_t* wall
 /* Device layout summary without allocating: run axis, runs, plain bulk sites,
  * general sites (or an error if the lattice cannot be streamed exactly). */
 int hb_geometry_layout(const hb_geometry* g, const hb_params* params, int wall, int64_t stats[4]);
+/* FNV-1a digests of every array and scalar of the storage layout, built on the
+ * host (device < 0) or on that device: [0] scalars (n, halo, stride, axis, runs,
+ * bulk and general counts, bins, coupling total, closest directions), [1..16]
+ * st2ref, ref2st, meta, run offsets, and the general records' site, run,
+ * sources, iolet, coupling slot, coordinates, kind, wall and iolet masks,
+ * cut distances, normals, couplings; the rest 0.  Both builds give the same
+ * digests for every lattice (a check of the device passes). */
+int hb_geometry_layout_digest(const hb_geometry* g, const hb_params* params, int wall, int device, uint64_t digest[32]);
 /* The selector's site mask over the geometry (contiguous order; 1 = taken), for a
  * voxel size and origin in metres.  Host-only. */
 int hb_geometry_select(const hb_geometry* g, const hb_selector* sel, double voxel_size, const double origin[3],

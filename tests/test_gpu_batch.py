@@ -120,6 +120,23 @@ def test_prepared_admission_matches_and_survives_refusal(mix):
         assert np.array_equal(a, m)
 
 
+def test_prepared_on_the_device_matches(mix):
+    """A lattice decoded and laid out on the device steps as one prepared on the host."""
+    name, xml, kernel, wall, steps = mix[0]
+    out = []
+    for device in (None, 0):
+        prep = lbm.PreparedLattice(xml, kernel, wall, steps, device=device)
+        b = lbm.Batch(400_000, 200_000, 8)
+        slot = b.add_prepared(prep)
+        prep.close()
+        done = []
+        while not done:
+            done = b.run(64)
+        out.append(b.macro(slot))
+    for a, m in zip(*out):
+        assert np.array_equal(a, m)
+
+
 @pytest.mark.parametrize("tuning", [(1, 256, "split"), (2, 128, "split"), (2, 256, "persistent"),
                                     (1, 128, "persistent")])
 def test_every_launch_shape_gives_the_same_result(mix, tuning):

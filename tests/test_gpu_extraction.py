@@ -199,3 +199,48 @@ def test_selected_record_is_the_whole_record_restricted(case_dir, tmp_path):
         assert np.array_equal(coords, wcoords[mask])
         for f in fields:
             assert np.array_equal(vals[f], wvals[f][mask])
+
+
+def test_device_selection_is_byte_identical_to_host_selection(case_dir, tmp_path):
+    """Every selector type, selected and gathered on the device: the file equals,
+    byte for byte, the whole-lattice file restricted to the sites the host
+    selector (the reference's float arithmetic, hb_geometry_select) takes, with
+    macroscopic fields, stress caches and distributions."""
+    import struct as st
+    xml, gmy, info, kernel, wall, _ = make_small_case(case_dir, "pipe_bfl")
+    sim = lbm.LBM(xml, kernel=kernel, wall=wall)
+    sim.step(40, macro=True, stress=True)
+    fields = ["pressure", "velocity", "shearstress", "vonmisesstress", "stresstensor", "traction", "distributions"]
+    whole = tmp_path / "whole.xtr"
+    sim.WriteXtr(whole, fields)
+    w = read_xtr(whole)
+    raw = open(whole, "rb").read()
+    hdr = raw[:w["header_len"]]
+    per_site = 4 * (3 + sum(width for _, width, _ in w["fields"]))
+    body = raw[w["header_len"] + 8:]
+    label = raw[w["header_len"]:w["header_len"] + 8]
+    (_, wcoords, wvals), = w["records"]
+    dx = units(xml, kernel)[0]
+    lo, hi = wcoords.min(0), wcoords.max(0)
+    mid = (lo + hi) / 2.0 * dx
+    r = (hi[0] - lo[0]) / 2.0 * dx
+    wall_site = wcoords[np.flatnonzero(np.abs(wvals["shearstress"][:, 0]) < 1e30)[len(wcoords) // 100]] * dx
+    geo = lbm.Geometry(gmy)
+    sels = [lbm.selector("whole"),
+            lbm.selector("plane", point=mid, normal=(0, 0, 1)),
+            lbm.selector("plane", point=mid, normal=(0, 1, 1), radius=0.5 * r),
+            lbm.selector("line", point=lo * dx, point2=hi * dx),
+            lbm.selector("sphere", point=mid, radius=0.6 * r),
+            lbm.selector("inlet"), lbm.selector("outlet"), lbm.selector("surface"),
+            lbm.selector("surfaceWithinSphere", point=mid, radius=1.3 * r),
+            lbm.selector("surfacepoint", point=wall_site)]
+    for k, sel in enumerate(sels):
+        path = tmp_path / f"sel{k}.xtr"
+        sim.WriteXtr(path, fields, geometry=sel)
+        mask = geo.select(sel, dx, (0.0, 0.0, 0.0))
+        assert mask.any(), k
+        expect = bytearray(hdr)
+        expect[44:52] = st.pack(">Q", int(mask.sum()))
+        rows = [body[j * per_site:(j + 1) * per_site] for j in np.flatnonzero(mask)]
+        expect += label + b"".join(rows)
+        assert open(path, "rb").read() == bytes(expect), (k, sel.type)
