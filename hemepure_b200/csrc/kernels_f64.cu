@@ -28,7 +28,7 @@
 namespace hb {
 namespace {
 
-constexpr int kGeneralBlocksPerSM = 5;
+constexpr int kGeneralBlocksPerSM = 4;
 
 // ---------------------------------------------------------------------------
 // Kernels
@@ -48,12 +48,14 @@ __global__ void __launch_bounds__(256, (is_sponge(K) || MACRO) ? 1 : 3) k_bulk(c
 }
 
 // The boundary kernel is latency-bound.  Its gather issues the eighteen loads
-// of a record together (f64_site.cuh), which needs the registers to hold them:
-// with LBGK or TRT, bounce-back or BFL walls and no outputs it is held to 96
-// registers, five blocks of 128 per SM (4M-site pipe, time alone: 64 registers
-// 0.0628 ms with spills, 80 registers 0.0571 ms, 96 registers 0.0553 ms; the
-// whole step 0.2298 / 0.2231 / 0.2215 ms).  The sponge-layer kernels, GZS walls
-// and output steps keep the compiler's allocation.
+// of a record together with the BFL cut distances and own-site values
+// (f64_site.cuh), which needs the registers to hold them: with LBGK or TRT,
+// bounce-back or BFL walls and no outputs it runs four blocks of 128 per SM
+// (125 registers).  4M-site pipe, time alone / whole step: five blocks (96
+// registers, 88 bytes spilled) 0.0523 / 0.2233 ms, four blocks 0.0429 / 0.2171
+// ms; with the BFL loads issued link by link, five blocks 0.0545 / 0.2219 ms and
+// four 0.0585 / 0.2261 ms.  The sponge-layer kernels, GZS walls and output steps
+// keep the compiler's allocation.
 template <int K, int WALL, bool GATHER, bool MACRO>
 __global__ void __launch_bounds__(128, (!is_sponge(K) && WALL != kGZS && !MACRO) ? kGeneralBlocksPerSM : 1)
     k_general(const StepArgs a) {

@@ -143,10 +143,13 @@ __global__ void __launch_bounds__(256) k_bulk_lp(const StepArgs a, const MixArgs
 }
 
 // The boundary kernel is latency-bound: outside the LES kernel, GZS walls and
-// output steps it is held to 64 registers (eight blocks of 128 per SM; its own
-// allocation is 68-72), measured 30.3k -> 30.7k MLUPS for the FP32 step on the 4M pipe.
+// output steps it runs six blocks of 128 per SM (up to 80 registers), which
+// holds the gather and the BFL loads in flight together (mixed_site.cuh).
+// FP32 on the 4M pipe, time alone / whole step: eight blocks 0.0355 / 0.1231
+// ms, six 0.0326 / 0.1211 ms, five 0.0336 / 0.1227 ms; with the BFL loads
+// issued link by link and eight blocks, 0.0428 / 0.1252 ms.
 template <class S, int K, int WALL, bool GATHER, bool MACRO>
-__global__ void __launch_bounds__(128, (K != kLES && WALL != kGZS && !MACRO) ? 8 : 1)
+__global__ void __launch_bounds__(128, (K != kLES && WALL != kGZS && !MACRO) ? 6 : 1)
     k_general_m(const StepArgs a, const MixArgs m) {
   const int gi = blockIdx.x * blockDim.x + threadIdx.x;
   if (gi >= a.gen.G) return;

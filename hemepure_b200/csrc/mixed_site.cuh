@@ -246,21 +246,24 @@ __device__ __forceinline__ void gather_general_m(const StepArgs& a, const MixArg
     g[i] = v;
   }
   if (WALL == kBFL && wm) {
+    // The BFL rule of gather_general (f64_site.cuh), in FP32 on the stored
+    // deviations; cut distances and own-site values loaded before any arithmetic.
+    float qv[18], fo[18];
 #pragma unroll
     for (int i = 1; i < Q; i++) {
       const int d = inv(i);
-      if (((wm >> (d - 1)) & 1u) && !((wm >> (i - 1)) & 1u) && !((im >> (d - 1)) & 1u)) {
-        const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
-        const float fi = ldg_s<S>(m, (int64_t)i * a.np + s);
-        if (!(q < 0.5f)) g[i] = (g[i] + (2.0f * q - 1.0f) * fi) / (2.0f * q);
-      }
+      const bool corr = ((wm >> (d - 1)) & 1u) && !((wm >> (i - 1)) & 1u);
+      qv[i - 1] = corr ? __ldg(G.q + (int64_t)(d - 1) * G.G + gi) : 1.0f;
+      fo[i - 1] = corr ? ldg_s<S>(m, (int64_t)i * a.np + s) : 0.0f;
     }
 #pragma unroll
-    for (int d = 1; d < Q; d++) {
-      const int i = inv(d);
-      if (((wm >> (d - 1)) & 1u) && !((wm >> (i - 1)) & 1u)) {
-        const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
-        if (q < 0.5f) g[i] = 2.0f * q * g[i] + (1.0f - 2.0f * q) * g[d];
+    for (int i = 1; i < Q; i++) {
+      const int d = inv(i);
+      const bool corr = ((wm >> (d - 1)) & 1u) && !((wm >> (i - 1)) & 1u);
+      if (corr) {
+        const float q = qv[i - 1];
+        if (!(q < 0.5f)) g[i] = (g[i] + (2.0f * q - 1.0f) * fo[i - 1]) / (2.0f * q);
+        else g[i] = 2.0f * q * g[i] + (1.0f - 2.0f * q) * g[d];
       }
     }
   }
