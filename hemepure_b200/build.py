@@ -32,7 +32,7 @@ CU_SOURCES = {
     "extract.cu": ["-fmad=false"],
 }
 CPP_SOURCES = ["xml.cpp", "config.cpp", "layout.cpp", "shard.cpp", "solver.cpp", "extraction.cpp", "batch.cpp", "capi.cpp"]
-HEADERS = ["hb_common.h", "f64_site.cuh", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h", "mixed_site.cuh", "batch.h", "batch_dev.h", "shard.h"]
+HEADERS = ["hb_common.h", "f64_site.cuh", "xml.h", "config.h", "layout.h", "device.h", "solver.h", "extraction.h", "mixed_site.cuh", "batch.h", "batch_dev.h", "shard.h", "setup_pool.h"]
 
 
 def _deps_mtime() -> float:

@@ -16,6 +16,10 @@
 struct hb_handle {
   std::unique_ptr<hb::Solver> solver;
   std::string error;
+  // Wall-clock ms of hb_create_from_xml's phases: case file, geometry decode
+  // (and, with the device reader, the layout and the tables' copy back), the
+  // solver's construction (layout when not built already, uploads, initial state).
+  double setup_ms[4] = {0, 0, 0, 0};
 };
 
 struct hb_geometry {
@@ -83,15 +87,27 @@ int hb_create_from_xml(const char* xml_path, const hb_options* opt, hb_handle** 
     hb_options o;
     hb_default_options(&o);
     if (opt) o = *opt;
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
     hb::CaseConfig c = hb::read_case(xml_path, o.kernel);
+    const auto t1 = clk::now();
     // The device reader also lays the lattice out on the device.
     hb::Layout L;
     const bool dev = o.geometry_reader == HB_GEOMETRY_DEVICE;
     if (dev) hb::validate_case(c.params, o);
     hb::LatticeTables t = dev ? hb::read_gmy_device(c.gmy_path, o.device, nullptr, &c.params, o.wall, &L)
                               : hb::read_gmy(c.gmy_path);
+    const auto t2 = clk::now();
     int rc = finish_create(std::move(t), c.params, o, out, dev ? &L : nullptr);
-    if (rc == HB_OK) (*out)->solver->set_units(c.dt, c.dx, c.origin);
+    if (rc == HB_OK) {
+      (*out)->solver->set_units(c.dt, c.dx, c.origin);
+      const auto t3 = clk::now();
+      auto ms = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+      (*out)->setup_ms[0] = ms(t0, t1);
+      (*out)->setup_ms[1] = ms(t1, t2);
+      (*out)->setup_ms[2] = ms(t2, t3);
+      (*out)->setup_ms[3] = ms(t0, t3);
+    }
     if (rc == HB_OK && !c.checkpoint_file.empty()) {
       std::string cp = c.checkpoint_file;
       if (!cp.empty() && cp[0] != '/') {
@@ -744,6 +760,12 @@ int hb_geometry_layout_digest(const hb_geometry* g, const hb_params* params, int
 int hb_geometry_close(hb_geometry* g) {
   if (!g) return HB_ERR_ARG;
   delete g;
+  return HB_OK;
+}
+
+int hb_setup_timing(const hb_handle* h, double ms[4]) {
+  if (!h || !ms) return HB_ERR_ARG;
+  for (int k = 0; k < 4; k++) ms[k] = h->setup_ms[k];
   return HB_OK;
 }
 

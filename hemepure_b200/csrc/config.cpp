@@ -15,6 +15,9 @@
 // 800-946 (inflate, site records); classification src/geometry/SiteDataBare.cc:24-172;
 // site order src/geometry/LatticeData.cc:69-285 and LatticeData.h:375-436;
 // neighbour table src/geometry/LatticeData.cc:366-443.
+#include <sys/mman.h>
+
+#include <cstdlib>
 #include "config.h"
 
 #include <zlib.h>
@@ -441,6 +444,22 @@ struct ReadSite {
 };
 
 }  // namespace
+
+void* host_table_alloc(size_t bytes) {
+  constexpr size_t kHuge = (size_t)2 << 20;
+  if (bytes < 8 * kHuge) {
+    void* p = std::malloc(bytes);
+    if (!p) throw std::bad_alloc();
+    return p;
+  }
+  const size_t rounded = (bytes + kHuge - 1) / kHuge * kHuge;
+  void* p = std::aligned_alloc(kHuge, rounded);
+  if (!p) throw std::bad_alloc();
+  madvise(p, rounded, MADV_HUGEPAGE);  // advice only: ignored where huge pages are off
+  return p;
+}
+
+void host_table_free(void* p) { std::free(p); }
 
 LatticeTables read_gmy(const std::string& path) {
   std::ifstream in(path, std::ios::binary);

@@ -2,8 +2,10 @@
 // lattice tables of one rank (the reference's geometry::LatticeData).
 #pragma once
 
+#include <algorithm>
 #include <complex>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -37,6 +39,86 @@ struct CaseConfig {
 // which kernel-specific elements are required, as HEMELB_KERNEL does.
 CaseConfig read_case(const std::string& xml_path, int kernel);
 
+// A host array of plain values whose resize leaves new elements unset: the
+// large site tables (coordinates, cut distances, normals: 124 bytes a site) are
+// written in full by whoever fills them, and a zero fill first would cost as
+// much as the copy from the device.  Large arrays are aligned to 2 MiB and
+// advised as huge-page candidates, so that first touching them takes a few
+// hundred page faults instead of a hundred thousand.  The subset of std::vector
+// the tables use.
+void* host_table_alloc(size_t bytes);
+void host_table_free(void* p);
+
+template <class T>
+class HostArray {
+ public:
+  using value_type = T;
+  HostArray() = default;
+  HostArray(const HostArray& o) { assign(o.begin(), o.end()); }
+  HostArray(HostArray&& o) noexcept : p_(o.p_), n_(o.n_) {
+    o.p_ = nullptr;
+    o.n_ = 0;
+  }
+  HostArray& operator=(const HostArray& o) {
+    if (this != &o) assign(o.begin(), o.end());
+    return *this;
+  }
+  HostArray& operator=(HostArray&& o) noexcept {
+    if (this != &o) {
+      host_table_free(p_);
+      p_ = o.p_;
+      n_ = o.n_;
+      o.p_ = nullptr;
+      o.n_ = 0;
+    }
+    return *this;
+  }
+  ~HostArray() { host_table_free(p_); }
+
+  size_t size() const { return n_; }
+  bool empty() const { return n_ == 0; }
+  T* data() { return p_; }
+  const T* data() const { return p_; }
+  T* begin() { return p_; }
+  T* end() { return p_ + n_; }
+  const T* begin() const { return p_; }
+  const T* end() const { return p_ + n_; }
+  T& operator[](size_t k) { return p_[k]; }
+  const T& operator[](size_t k) const { return p_[k]; }
+  void clear() {
+    host_table_free(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+  // New elements are left unset; old ones are kept.
+  void resize(size_t n) {
+    if (n == n_) return;
+    T* q = n ? static_cast<T*>(host_table_alloc(n * sizeof(T))) : nullptr;
+    for (size_t k = 0; k < std::min(n, n_); k++) q[k] = p_[k];
+    host_table_free(p_);
+    p_ = q;
+    n_ = n;
+  }
+  template <class It>
+  void assign(It first, It last) {
+    const size_t n = (size_t)(last - first);
+    T* q = n ? static_cast<T*>(host_table_alloc(n * sizeof(T))) : nullptr;
+    for (size_t k = 0; k < n; k++) q[k] = (T)first[k];
+    host_table_free(p_);
+    p_ = q;
+    n_ = n;
+  }
+  void assign(size_t n, T v) {
+    clear();
+    resize(n);
+    for (size_t k = 0; k < n; k++) p_[k] = v;
+  }
+
+ private:
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
 // Lattice tables in the reference's contiguous order
 // (src/geometry/LatticeData.cc:69-285, 366-443; LatticeData.h:375-436).
 struct LatticeTables {
@@ -45,13 +127,13 @@ struct LatticeTables {
   int64_t block_size = 0;
   int64_t blocks[3] = {0, 0, 0};
   int64_t type_counts[6] = {0, 0, 0, 0, 0, 0};
-  std::vector<int64_t> coords;      // [n*3]
+  HostArray<int64_t> coords;        // [n*3]
   std::vector<uint32_t> wall;       // [n]
   std::vector<uint32_t> iolet;      // [n]
   std::vector<int32_t> stype;       // [n] 0 fluid 1 inlet 2 outlet
   std::vector<int32_t> iolet_id;    // [n]
-  std::vector<float> q;             // [n*18] cut distances as the .gmy stores them (float; -1 no wall link)
-  std::vector<float> normal;        // [n*3] wall normal, normalised in float (HUGE_VALF without one)
+  HostArray<float> q;               // [n*18] cut distances as the .gmy stores them (float; -1 no wall link)
+  HostArray<float> normal;          // [n*3] wall normal, normalised in float (HUGE_VALF without one)
   std::vector<int64_t> nbr;         // [n*19] neighbourIndices, or empty: derived from the coordinates
                                     // when asked for (neighbour_table)
   // One slab of a sharded lattice: sites [0, n_owned) are this shard's own, in

@@ -318,7 +318,7 @@ void write_xtr(Solver& s, const std::string& path, const std::string& fields_csv
   // signed zeros and the non-finite normals of sites off the wall come out as the
   // reference's conversions give them.
   constexpr double kRefPressureMmHg = 0.0;
-  const std::vector<float>& normal = t.normal;
+  const HostArray<float>& normal = t.normal;
 
   XdrOut hdr;
   {

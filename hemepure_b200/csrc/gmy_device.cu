@@ -35,12 +35,15 @@
 #include <chrono>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
 #include "config.h"
 #include "layout.h"
+#include "setup_pool.h"
 
 namespace hb {
 namespace {
@@ -256,23 +259,6 @@ __global__ void k_place(const BlockDev* __restrict__ blocks, int nb, const int64
   }
 }
 
-// Device allocations of one read, freed on every path.
-struct Pool {
-  std::vector<void*> ptrs;
-  ~Pool() {
-    for (void* p : ptrs) cudaFree(p);
-  }
-  template <class T>
-  T* get(size_t count) {
-    void* p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(T));
-    if (e != cudaSuccess)
-      throw Error{e == cudaErrorMemoryAllocation ? HB_ERR_OOM : HB_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
-    ptrs.push_back(p);
-    return static_cast<T*>(p);
-  }
-};
-
 void cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw Error{HB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 }
@@ -286,6 +272,25 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 }
 
 }  // namespace
+
+cudaMemPool_t setup_pool(int device, bool fresh) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(device);
+  if (it != pools.end() && !fresh) return it->second;
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  cuda_check(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+  uint64_t keep = kSetupPoolKeep;
+  cuda_check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+  pools[device] = pool;
+  return pool;
+}
 
 LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* timing, const hb_params* params, int wall,
                               Layout* layout) {
@@ -371,7 +376,7 @@ LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* ti
     cudaStream_t s;
     ~StreamGuard() { cudaStreamDestroy(s); }
   } sg{st};
-  Pool P;
+  SetupPool P(device, st);
   auto t2 = std::chrono::steady_clock::now();
   uint32_t* d_raw = P.get<uint32_t>(raw_size / 4 + 1);
   BlockDev* d_blocks = P.get<BlockDev>(nb);
@@ -461,18 +466,53 @@ LatticeTables read_gmy_device(const std::string& path, int device, GmyTiming* ti
       d2h_err = cudaErrorMemoryAllocation;
       return;
     }
-    auto copy = [&](void* dst, const void* src, size_t bytes) {
-      if (d2h_err == cudaSuccess) d2h_err = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st2);
+    // Pageable copies go through the driver's staging buffers and the host's
+    // first touch of each page: a few host threads, each with its own stream and
+    // a slice of every table, keep the copy engine busy.
+    struct Part {
+      void* dst;
+      const void* src;
+      size_t bytes, elem;
     };
-    copy(t.coords.data(), T.coords, t.coords.size() * sizeof(int64_t));
-    copy(t.wall.data(), T.wall, n * sizeof(uint32_t));
-    copy(t.iolet.data(), T.iolet, n * sizeof(uint32_t));
-    copy(t.stype.data(), T.stype, n * sizeof(int32_t));
-    copy(t.iolet_id.data(), T.iolet_id, n * sizeof(int32_t));
-    copy(t.q.data(), T.q, t.q.size() * sizeof(float));
-    copy(t.normal.data(), T.normal, t.normal.size() * sizeof(float));
-    const cudaError_t e = cudaStreamSynchronize(st2);
-    if (d2h_err == cudaSuccess) d2h_err = e;
+    const Part parts[] = {{t.coords.data(), T.coords, t.coords.size() * sizeof(int64_t), sizeof(int64_t)},
+                          {t.wall.data(), T.wall, (size_t)n * sizeof(uint32_t), sizeof(uint32_t)},
+                          {t.iolet.data(), T.iolet, (size_t)n * sizeof(uint32_t), sizeof(uint32_t)},
+                          {t.stype.data(), T.stype, (size_t)n * sizeof(int32_t), sizeof(int32_t)},
+                          {t.iolet_id.data(), T.iolet_id, (size_t)n * sizeof(int32_t), sizeof(int32_t)},
+                          {t.q.data(), T.q, t.q.size() * sizeof(float), sizeof(float)},
+                          {t.normal.data(), T.normal, t.normal.size() * sizeof(float), sizeof(float)}};
+    const int workers = (int)std::max<int64_t>(1, std::min<int64_t>(nthreads, n / 65536));
+    std::vector<cudaError_t> errs(workers, cudaSuccess);
+    auto work_slice = [&](int w) {
+      cudaError_t e = cudaSetDevice(device);
+      cudaStream_t ws = st2;
+      if (e == cudaSuccess && w > 0) e = cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking);
+      if (e != cudaSuccess) {
+        errs[w] = e;
+        return;
+      }
+      for (const Part& p : parts) {
+        const size_t count = p.bytes / p.elem;
+        const size_t b = count * w / workers, en = count * (w + 1) / workers;
+        // First touch of this slice's pages here, in parallel with the other
+        // workers, rather than inside the driver's copy.
+        volatile char* c = static_cast<char*>(p.dst);
+        for (size_t off = b * p.elem; off < en * p.elem; off += 4096) c[off] = 0;
+        if (en > b && e == cudaSuccess)
+          e = cudaMemcpyAsync(static_cast<char*>(p.dst) + b * p.elem, static_cast<const char*>(p.src) + b * p.elem,
+                              (en - b) * p.elem, cudaMemcpyDeviceToHost, ws);
+      }
+      const cudaError_t se = cudaStreamSynchronize(ws);
+      if (e == cudaSuccess) e = se;
+      if (w > 0) cudaStreamDestroy(ws);
+      errs[w] = e;
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < workers; w++) pool.emplace_back(work_slice, w);
+    work_slice(0);
+    for (auto& th : pool) th.join();
+    for (cudaError_t e : errs)
+      if (d2h_err == cudaSuccess) d2h_err = e;
   };
   if (!layout) {
     download();

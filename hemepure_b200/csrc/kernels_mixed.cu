@@ -49,9 +49,14 @@ __global__ void __launch_bounds__(256) k_bulk_m2(const StepArgs a, const MixArgs
 // M = sum c G,
 //   geq_i = w_i (D - 3/2 |M|^2 / (kScale + D) + 9/2 (c_i.M)^2 / (kScale + D) + 3 c_i.M),
 // which is kScale times the unscaled equilibrium of kernels_mixed.cu's header.
-// Opposite directions share the even part of the equilibrium.  4M-site pipe,
-// FP16 bulk kernel 0.0963 -> 0.0850 ms (0.45 -> 0.51 of the measured copy
-// bandwidth), the whole FP16 step 33.1k -> 36.1k MLUPS.
+// Opposite directions share the even part of the equilibrium.  The kernel is
+// issue-bound (about 460 instructions a site), so the positivity check compares
+// each value with its constant threshold (one predicated compare; NaN fails it
+// as before) and the stores walk one pointer by the plane stride.  4M-site
+// pipe, FP16 bulk kernel 0.0963 -> 0.0850 ms with the plane offsets, 0.0817 ms
+// with the trimmed check and stores (0.45 -> 0.52 of the measured copy
+// bandwidth), the whole FP16 step 33.1k -> 37.6k MLUPS.  Three sites per thread
+// measured slower (0.0903 ms).
 template <class S>
 struct Lp;
 template <>
@@ -79,7 +84,7 @@ __device__ __forceinline__ void collide_scaled(const StepArgs& a, const MixArgs&
     Mx += (float)cx(i) * G[i];
     My += (float)cy(i) * G[i];
     Mz += (float)cz(i) * G[i];
-    bad |= !(wf(i) * Lp<S>::kScale + G[i] > 0.0f);
+    bad |= !(G[i] > -wf(i) * Lp<S>::kScale);
   }
   if (bad) atomicOr(a.status, kStatusUnstable);
   const float inv = 1.0f / (Lp<S>::kScale + D);
@@ -105,8 +110,12 @@ __device__ __forceinline__ void collide_scaled(const StepArgs& a, const MixArgs&
       Lp<S>::st(m.fout, (int64_t)(i + 1) * a.np + s, G[i + 1] + sym - asym);
     }
   } else {
+    S* o = static_cast<S*>(m.fout) + s;
 #pragma unroll
-    for (int i = 0; i < Q; i++) Lp<S>::st(m.fout, (int64_t)i * a.np + s, G[i] + om * neq[i]);
+    for (int i = 0; i < Q; i++) {
+      Lp<S>::st(o, 0, G[i] + om * neq[i]);
+      o += a.np;
+    }
   }
 }
 
@@ -182,7 +191,7 @@ void launch_m4(const StepArgs& a, const MixArgs& m, int which, cudaStream_t st) 
     // 4M pipe), and keeping FP32 on the general kernel's arithmetic keeps a sharded
     // FP32 lattice bit-identical to the single lattice.
     if (GATHER && !MACRO && (K == kLBGK || K == kTRT) && a.run_po && sizeof(S) == 2)
-      k_bulk_lp<S, (K == kTRT ? kTRT : kLBGK), 2><<<(a.n + 511) / 512, 256, 0, st>>>(a, m);
+      k_bulk_lp<S, (K == kTRT ? kTRT : kLBGK), 2><<<(a.n + 256 * 2 - 1) / (256 * 2), 256, 0, st>>>(a, m);
     else if (GATHER && sizeof(S) == 2) k_bulk_m2<S, K, MACRO><<<(a.n + 511) / 512, 256, 0, st>>>(a, m);
     else k_bulk_m<S, K, GATHER, MACRO><<<(a.n + 255) / 256, 256, 0, st>>>(a, m);
   }

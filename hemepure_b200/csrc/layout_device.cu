@@ -26,6 +26,7 @@
 
 #include "hb_common.h"
 #include "layout.h"
+#include "setup_pool.h"
 
 namespace hb {
 namespace {
@@ -299,23 +300,6 @@ void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw Error{HB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 }
 
-// Device allocations of one build, freed on every path.
-struct Pool {
-  std::vector<void*> ptrs;
-  ~Pool() {
-    for (void* p : ptrs) cudaFree(p);
-  }
-  template <class T>
-  T* get(size_t count) {
-    void* p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(T));
-    if (e != cudaSuccess)
-      throw Error{e == cudaErrorMemoryAllocation ? HB_ERR_OOM : HB_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
-    ptrs.push_back(p);
-    return static_cast<T*>(p);
-  }
-};
-
 template <class T>
 void download(std::vector<T>& out, const T* src, size_t count, cudaStream_t st) {
   out.resize(count);
@@ -362,7 +346,9 @@ Layout layout_on_device(const DeviceTables& d, const hb_params& p, void* stream)
   L.n_halo = (int)(nt - n);
   L.np = ((nt + 63) / 64) * 64;
 
-  Pool P;
+  int device = 0;
+  check(cudaGetDevice(&device), "cudaGetDevice");
+  SetupPool P(device, st);
   int* err = P.get<int>(2);
   int herr[2] = {0, 0};
   auto sync_and_check = [&](const char* what) {
@@ -519,7 +505,7 @@ Layout build_layout_on_device(const LatticeTables& t, const hb_params& p, int wa
     cudaStream_t s;
     ~StreamGuard() { cudaStreamDestroy(s); }
   } sg{st};
-  Pool P;
+  SetupPool P(device, st);
   const int64_t n = t.n;
   DeviceTables d;
   d.n = n;

@@ -41,7 +41,7 @@ EXPORTS = [
     "hb_request_comms", "hb_pre_send", "hb_pre_receive", "hb_post_receive", "hb_end_iteration",
     "hb_step", "hb_site_count", "hb_time_step", "hb_get_params", "hb_get_fs", "hb_set_fs",
     "hb_get_macro", "hb_get_stress", "hb_set_iolet_densities", "hb_get_wk3", "hb_get_tables", "hb_write_xtr", "hb_read_checkpoint",
-    "hb_last_step_timing", "hb_device_bytes", "hb_read_case", "hb_geometry_open", "hb_geometry_site_count",
+    "hb_last_step_timing", "hb_setup_timing", "hb_device_bytes", "hb_read_case", "hb_geometry_open", "hb_geometry_site_count",
     "hb_geometry_tables", "hb_geometry_layout", "hb_geometry_layout_digest", "hb_geometry_close", "hb_profile_steps",
     "hb_set_time_step", "hb_moment_sums", "hb_moment_sums_noalloc",
     "hb_batch_bytes", "hb_batch_create", "hb_batch_destroy", "hb_batch_add_xml", "hb_batch_add", "hb_batch_remove",
@@ -154,6 +154,7 @@ def library() -> C.CDLL:
     L.hb_iolet_velocity.argtypes = [C.POINTER(Iolet), P, U64, P]
     L.hb_read_checkpoint.argtypes = [P, C.c_char_p, U64]
     L.hb_last_step_timing.argtypes = [P, P, P]
+    L.hb_setup_timing.argtypes = [P, P]
     L.hb_device_bytes.argtypes = [P, P]
     L.hb_read_case.argtypes = [C.c_char_p, I, P, C.c_char_p, C.c_size_t]
     L.hb_geometry_open.argtypes = [C.c_char_p, C.POINTER(P)]
@@ -423,6 +424,13 @@ class LBM:
 
     def ReadCheckpoint(self, path: str, step: int = 0) -> None:
         self._check(library().hb_read_checkpoint(self._h, os.fspath(path).encode(), int(step)))
+
+    def setup_timing(self) -> Dict[str, float]:
+        """Wall-clock ms of the construction from a case file: case, geometry
+        (decode, layout, tables back), solver (uploads, initial state), total."""
+        ms = np.zeros(4)
+        self._check(library().hb_setup_timing(self._h, _p(ms)))
+        return {"case": float(ms[0]), "geometry": float(ms[1]), "solver": float(ms[2]), "total": float(ms[3])}
 
     def last_step_timing(self):
         ms = C.c_double()

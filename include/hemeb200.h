@@ -473,6 +473,11 @@ int hb_moment_sums_noalloc(const double* f, int64_t dir_stride, int64_t site_str
 /* Device-time of the last hb_step call's kernels in milliseconds (CUDA events),
  * and the number of kernel launches it made. */
 int hb_last_step_timing(const hb_handle* h, double* ms, int64_t* launches);
+/* Wall-clock milliseconds of hb_create_from_xml's phases: ms[0] the case file,
+ * ms[1] the geometry (with the device reader: decode, layout and the tables'
+ * copy back), ms[2] the solver (uploads, initial state), ms[3] the total;
+ * zeros for a handle made another way. */
+int hb_setup_timing(const hb_handle* h, double ms[4]);
 /* Advance 2 x `n_steps` steps with CUDA events around the launches (for
  * measurement only).  The first n_steps run as hb_step runs them and ms[0]
  * sums their collide-and-stream launch (one fused kernel, or the bulk and
