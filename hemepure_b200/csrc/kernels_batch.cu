@@ -60,9 +60,10 @@ __device__ __forceinline__ void relax_inplace(float* g, int* status, bool trt, f
 
 // Gather of a boundary record with the wall rule chosen at run time (SBB or
 // BFL); the rules are those of gather_general_m.  Every load depends only on
-// the record's metadata and run offsets, so all are in flight together: on a
-// BFL link the value at the site is read whether or not the cut distance
-// selects it.
+// the record's metadata and run offsets, and its address is chosen without a
+// branch (records of small vessels side by side in a warp have different link
+// masks), so all are in flight together; the BFL cut distances and own-site
+// values follow in one batch before any arithmetic.
 template <class S>
 __device__ __forceinline__ void gather_general_rt(const StepArgs& a, const MixArgs& m, int gi, int s, uint32_t wm,
                                                   uint32_t im, int run, const int* off, bool bfl, float* g) {
@@ -72,30 +73,27 @@ __device__ __forceinline__ void gather_general_rt(const StepArgs& a, const MixAr
   for (int i = 1; i < Q; i++) {
     const int d = inv(i);
     const bool bw = (wm >> (d - 1)) & 1u, bi = (im >> (d - 1)) & 1u;
-    if (bi) {
-      g[i] = __ldg(m.gin + (int64_t)(d - 1) * G.G + gi);
-    } else if (bw) {
-      const float fd = ldg_s<S>(m, (int64_t)d * a.np + s);
-      const bool wi = (wm >> (i - 1)) & 1u;
-      if (bfl && !wi) {
-        const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
-        const float fi = ldg_s<S>(m, (int64_t)i * a.np + s);
-        g[i] = q < 0.5f ? fd : (fd + (2.0f * q - 1.0f) * fi) / (2.0f * q);
-      } else {
-        g[i] = fd;
-      }
-    } else {
-      const int src = run >= 0 ? s + off[i] : __ldg(G.src + (int64_t)(i - 1) * G.G + gi);
-      g[i] = ldg_s<S>(m, (int64_t)i * a.np + src);
-    }
+    const int src = run >= 0 ? s + off[i] : __ldg(G.src + (int64_t)(i - 1) * G.G + gi);
+    const int64_t k = bw ? (int64_t)d * a.np + s : (int64_t)i * a.np + src;
+    g[i] = bi ? __ldg(m.gin + (int64_t)(d - 1) * G.G + gi) : ldg_s<S>(m, k);
   }
   if (bfl && wm) {
+    float qv[18], fo[18];
 #pragma unroll
-    for (int d = 1; d < Q; d++) {
-      const int i = inv(d);
-      if (((wm >> (d - 1)) & 1u) && !((wm >> (i - 1)) & 1u)) {
-        const float q = __ldg(G.q + (int64_t)(d - 1) * G.G + gi);
-        if (q < 0.5f) g[i] = 2.0f * q * g[i] + (1.0f - 2.0f * q) * g[d];
+    for (int i = 1; i < Q; i++) {
+      const int d = inv(i);
+      const bool corr = ((wm >> (d - 1)) & 1u) && !((wm >> (i - 1)) & 1u);
+      qv[i - 1] = corr ? __ldg(G.q + (int64_t)(d - 1) * G.G + gi) : 1.0f;
+      fo[i - 1] = corr ? ldg_s<S>(m, (int64_t)i * a.np + s) : 0.0f;
+    }
+#pragma unroll
+    for (int i = 1; i < Q; i++) {
+      const int d = inv(i);
+      const bool corr = ((wm >> (d - 1)) & 1u) && !((wm >> (i - 1)) & 1u);
+      if (corr) {
+        const float q = qv[i - 1];
+        if (!(q < 0.5f)) g[i] = (g[i] + (2.0f * q - 1.0f) * fo[i - 1]) / (2.0f * q);
+        else g[i] = 2.0f * q * g[i] + (1.0f - 2.0f * q) * g[d];
       }
     }
   }
@@ -220,8 +218,12 @@ __global__ void __launch_bounds__(256, SPT == 1 ? 6 : 3) k_batch_bulk(const Batc
   batch_bulk_tile<S, SPT>(b, m, blockIdx.x);
 }
 
+// Eight blocks of 128 per SM (64 registers, ~60 bytes spilled): with the
+// batched BFL loads, ten blocks (48 registers) spilled ~160 bytes; six (80
+// registers, none spilled) measured the same as eight.  Serving probe (11
+// requests, 8.1M sites): 28.9k -> 30.3k MLUPS for the split step form.
 template <class S>
-__global__ void __launch_bounds__(128, 10) k_batch_gen(const BatchArgs b) {
+__global__ void __launch_bounds__(128, 8) k_batch_gen(const BatchArgs b) {
   const MixArgs m{b.fin, b.fout, b.gin, b.gout};
   batch_general_tile<S>(b, m, blockIdx.x);
 }

@@ -231,6 +231,9 @@ class Server:
         # Per block: wall seconds since the previous block ended (host work
         # included), site updates made, members resident at its start.
         self.block_log: List[Tuple[float, float, int]] = []
+        # Host wall seconds: inside batch.run (launch, graph capture when the
+        # membership changed, the wait), admissions, retirements.
+        self.host_s = {"run": 0.0, "admit": 0.0, "retire": 0.0}
 
     def submit(self, r: Request) -> None:
         self.prepared[r.rid] = self.pool.submit(lbm.PreparedLattice, r.xml, r.kernel, r.wall, r.steps)
@@ -274,7 +277,9 @@ class Server:
                 now = clock() - t0
                 while pending and pending[0].arrival <= now:
                     self.submit(pending.popleft())
+                ta = clock()
                 self._admit(now)
+                self.host_s["admit"] += clock() - ta
                 if not self.running:
                     if pending and not self.queue:
                         time.sleep(max(0.0, min(0.05, pending[0].arrival - (clock() - t0))))
@@ -286,13 +291,15 @@ class Server:
                     k = min(self.block_steps, r.steps - r.steps_done)
                     r.steps_done += k
                     updates += r.sites * k
+                tr = clock()
                 done = self.batch.run(self.block_steps)
+                self.host_s["run"] += clock() - tr
                 ms = self.batch.stats()[0]
                 self.device_ms += ms
                 self.blocks += 1
                 now = clock() - t0
                 self.block_log.append((now - last_end, float(updates), resident))
-                last_end = now
+                tt = clock()
                 for slot in done:
                     r = self.running.pop(slot)
                     n, t, st = self.batch.info(slot)
@@ -307,6 +314,8 @@ class Server:
                     r.finished = now
                     self.batch.remove(slot)
                     self.completed.append(r)
+                self.host_s["retire"] += clock() - tt
+                last_end = now
         finally:
             self.pool.shutdown(wait=True)
         self.wall_s = clock() - t0
@@ -339,7 +348,8 @@ class Server:
                 "aggregate_MLUPS": work / self.wall_s / 1e6, "wall_s": self.wall_s,
                 "device_busy_MLUPS": self.site_updates / (self.device_ms * 1e-3) / 1e6 if self.device_ms else 0.0,
                 "device_busy_fraction": self.device_ms * 1e-3 / self.wall_s if self.wall_s else 0.0,
-                "blocks": self.blocks, "site_capacity": self.site_capacity, "failed": len(failed),
+                "blocks": self.blocks, "host_s": dict(self.host_s), "device_s": self.device_ms * 1e-3,
+                "site_capacity": self.site_capacity, "failed": len(failed),
                 "failed_requests": [{"rid": r.rid, "status": r.status, "shape": r.shape, "sites": r.sites}
                                     for r in failed]}
 
@@ -372,7 +382,8 @@ def sustained_rate(requests: Sequence[Request], budget_bytes: int, tuning: Optio
     return {"MLUPS": sum(b[1] for b in sat) / wall / 1e6 if wall > 0 else rep["aggregate_MLUPS"],
             "saturated_blocks": len(sat), "saturated_wall_s": wall, "peak_resident": peak,
             "whole_pass_MLUPS": rep["aggregate_MLUPS"], "requests": len(reqs), "wall_s": rep["wall_s"],
-            "device_busy_MLUPS": rep["device_busy_MLUPS"]}
+            "device_busy_MLUPS": rep["device_busy_MLUPS"], "host_s": rep["host_s"], "device_s": rep["device_s"],
+            "blocks": rep["blocks"]}
 
 
 def solve_sequential_fp64(requests: Sequence[Request], device: int = 0) -> Dict[str, float]:
