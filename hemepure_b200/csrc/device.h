@@ -43,6 +43,7 @@ struct WK3Dev {           // InOutLetWK3 / InOutLetWK2 state
 
 struct GeneralDev {
   int G;
+  int G_noiolet;          // records [0, G_noiolet) have no iolet links (the first two collision-type bins)
   const int* site;        // [G] storage index
   const int* run;         // [G] run whose offsets the bulk slots follow, or -1
   const uint32_t* wall;   // [G] wall-link mask (bit d-1 for direction d)

@@ -264,10 +264,10 @@ __device__ __forceinline__ void load_run_offsets(const StepArgs& a, int r, int* 
 // links follows as a predicated step.  (4M-site pipe, boundary kernel alone:
 // branching per link 0.0599 ms, pull table for every record 0.0554 ms, run
 // offsets where they apply 0.0541 ms.)
-template <int WALL>
+template <int WALL, bool IO = true>
 __device__ __forceinline__ void gather_general(const StepArgs& a, int g, int s, double* f) {
   const GeneralDev& G = a.gen;
-  const uint32_t wm = __ldg(G.wall + g), im = __ldg(G.iolet + g);
+  const uint32_t wm = __ldg(G.wall + g), im = IO ? __ldg(G.iolet + g) : 0u;
   int src[18];
   const int run = __ldg(G.run + g);
   if (run >= 0) {
@@ -377,13 +377,13 @@ __device__ __forceinline__ void bulk_site_f64(const StepArgs& a, int s, int r) {
 }
 
 // One general (boundary or irregular) site record g.
-template <int K, int WALL, bool GATHER, bool MACRO>
+template <int K, int WALL, bool GATHER, bool MACRO, bool IO = true>
 __device__ __forceinline__ void general_site_f64(const StepArgs& a, int g) {
   const GeneralDev& G = a.gen;
   const int s = __ldg(G.site + g);
-  const uint32_t wm = __ldg(G.wall + g), im = __ldg(G.iolet + g);
+  const uint32_t wm = __ldg(G.wall + g), im = IO ? __ldg(G.iolet + g) : 0u;
   double f[Q];
-  if (GATHER) gather_general<WALL>(a, g, s, f);
+  if (GATHER) gather_general<WALL, IO>(a, g, s, f);
   else {
 #pragma unroll
     for (int i = 0; i < Q; i++) f[i] = ld(a.fin + (int64_t)i * a.np + s);

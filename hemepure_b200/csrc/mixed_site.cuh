@@ -44,9 +44,26 @@ struct GeqF {
     nh = 4.5f * inv;
     t1 = drho - 1.5f * (mx * mx + my * my + mz * mz) * inv;
   }
+  __device__ __forceinline__ float mde(int i) const { return (float)cx(i) * mx + (float)cy(i) * my + (float)cz(i) * mz; }
+  // w_i (t1 + nh (c_i.m)^2) + w_i 3 (c_i.m), each operation rounded as written,
+  // so that all() below gives the same bits.
   __device__ __forceinline__ float operator()(int i) const {
-    const float mde = (float)cx(i) * mx + (float)cy(i) * my + (float)cz(i) * mz;
-    return wf(i) * (t1 + nh * mde * mde + 3.0f * mde);
+    const float e = mde(i);
+    const float even = __fmul_rn(wf(i), __fmaf_rn(__fmul_rn(nh, e), e, t1));
+    const float odd = __fmul_rn(wf(i), __fmul_rn(3.0f, e));
+    return __fadd_rn(even, odd);
+  }
+  // Every direction's value; opposite directions (i, i + 1) share the even part.
+  __device__ __forceinline__ void all(float* out) const {
+    out[0] = (*this)(0);
+#pragma unroll
+    for (int i = 1; i < Q; i += 2) {
+      const float e = mde(i);
+      const float even = __fmul_rn(wf(i), __fmaf_rn(__fmul_rn(nh, e), e, t1));
+      const float odd = __fmul_rn(wf(i), __fmul_rn(3.0f, e));
+      out[i] = __fadd_rn(even, odd);
+      out[i + 1] = __fsub_rn(even, odd);
+    }
   }
 };
 
@@ -207,6 +224,23 @@ __device__ __forceinline__ float ldg_s(const MixArgs& m, int64_t k) { return Sto
 
 template <class S>
 __device__ __forceinline__ void gather_bulk_m(const StepArgs& a, const MixArgs& m, int s, int r, float* g) {
+  if (a.run_po) {
+    // The run table's plane offsets i * np + run_off[i]: one add per load.
+    const int4* o4 = reinterpret_cast<const int4*>(a.run_po) + 5 * r;
+    int po[20];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      const int4 v = __ldg(o4 + k);
+      po[4 * k] = v.x;
+      po[4 * k + 1] = v.y;
+      po[4 * k + 2] = v.z;
+      po[4 * k + 3] = v.w;
+    }
+    const S* base = static_cast<const S*>(m.fin) + s;
+#pragma unroll
+    for (int i = 0; i < Q; i++) g[i] = Store<S>::load(base, po[i]);
+    return;
+  }
   int off[20];
   run_offsets(a, r, off);
   g[0] = ldg_s<S>(m, s);
@@ -284,13 +318,17 @@ __device__ __forceinline__ void gather_any_m(const StepArgs& a, const MixArgs& m
 __device__ __forceinline__ void flag_unstable_status(const float* g, int* status) {
   bool bad = false;
 #pragma unroll
-  for (int i = 0; i < Q; i++) bad |= !(wf(i) + g[i] > 0.0f);
+  for (int i = 0; i < Q; i++) bad |= !(g[i] > -wf(i));
   if (bad) atomicOr(status, kStatusUnstable);
 }
 
 __device__ __forceinline__ void flag_unstable_m(const StepArgs& a, const float* g) { flag_unstable_status(g, a.status); }
 
-// Collision and store of plain bulk site s from its pre-collision g.
+// Collision and store of plain bulk site s from its pre-collision g.  The bulk
+// kernels issue about 490 instructions a site for 152 bytes (FP32), so the
+// equilibrium is evaluated by pairs of opposite directions and the stores walk
+// one pointer (4M pipe, FP32 bulk kernel 0.1065 -> 0.1038 ms, 0.83 -> 0.85 of
+// the measured copy bandwidth).
 template <class S, int K, bool MACRO>
 __device__ __forceinline__ void bulk_collide_m(const StepArgs& a, const MixArgs& m, int s, const float* g) {
   flag_unstable_m(a, g);
@@ -298,15 +336,22 @@ __device__ __forceinline__ void bulk_collide_m(const StepArgs& a, const MixArgs&
   moments_g(g, drho, mx, my, mz);
   const GeqF geq(drho, mx, my, mz);
   float fneq[Q];
+  geq.all(fneq);
 #pragma unroll
-  for (int i = 0; i < Q; i++) fneq[i] = g[i] - geq(i);
+  for (int i = 0; i < Q; i++) fneq[i] = g[i] - fneq[i];
   float om = (float)a.omega, tau = (float)a.tau;
   if (K == kLES) {
     tau = les_tau_f(a, fneq, (float)__ldg(a.vtau + s));
     om = -1.0f / tau;
   }
+  {
+    S* o = static_cast<S*>(m.fout) + s;
 #pragma unroll
-  for (int i = 0; i < Q; i++) Store<S>::store(m.fout, (int64_t)i * a.np + s, collide_one_f<K>(a, g, fneq, om, i));
+    for (int i = 0; i < Q; i++) {
+      Store<S>::store(o, 0, collide_one_f<K>(a, g, fneq, om, i));
+      o += a.np;
+    }
+  }
   if (MACRO) {
     const float rho = 1.0f + drho;
     a.rho[s] = (double)rho;

@@ -153,8 +153,8 @@ void Solver::upload() {
   }
   upload_vec(meta_, L_.meta, tot);
   upload_vec(run_off_, L_.run_off, tot);
-  if (opt_.precision == HB_STORE_FP16 && (int64_t)Q * np < ((int64_t)1 << 31)) {
-    // Plane offsets for the FP16 bulk kernel: one address add per load.
+  if (opt_.precision != HB_STORE_FP64 && (int64_t)Q * np < ((int64_t)1 << 31)) {
+    // Plane offsets for the shifted forms' bulk gather: one address add per load.
     std::vector<int> po(L_.run_off.size(), 0);
     for (size_t r = 0; r < po.size() / 20; r++)
       for (int i = 0; i < Q; i++) po[r * 20 + i] = (int)((int64_t)i * np + L_.run_off[r * 20 + i]);
@@ -329,6 +329,7 @@ StepArgs Solver::args() const {
   a.run_off = run_off_.as<int>();
   a.run_po = run_po_.p ? run_po_.as<int>() : nullptr;
   a.gen.G = L_.G;
+  a.gen.G_noiolet = L_.kind_start[2];
   a.gen.site = g_site_.as<int>();
   a.gen.run = g_run_.as<int>();
   a.gen.wall = g_wall_.as<uint32_t>();

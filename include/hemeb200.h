@@ -473,7 +473,9 @@ int hb_moment_sums_noalloc(const double* f, int64_t dir_stride, int64_t site_str
 /* Device-time of the last hb_step call's kernels in milliseconds (CUDA events),
  * and the number of kernel launches it made. */
 int hb_last_step_timing(const hb_handle* h, double* ms, int64_t* launches);
-/* Wall-clock milliseconds of hb_create_from_xml's phases: ms[0] the case file,
+/* Replaces the set-up timers of reporting::Timers (fileRead, unzip,
+ * latDatInitialise; src/reporting/Timers.h:82-100).
+ * Wall-clock milliseconds of hb_create_from_xml's phases: ms[0] the case file,
  * ms[1] the geometry (with the device reader: decode, layout and the tables'
  * copy back), ms[2] the solver (uploads, initial state), ms[3] the total;
  * zeros for a handle made another way. */
