@@ -330,7 +330,7 @@ def main():
                 "traffic": traffic, "kernel": "k_bulk (plain bulk sites)", "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": bytes_per_site * lay["bulk_sites"], "launch_ms": bulk_launch_ms,
                 "boundary_kernel_alone_ms": g_ms / prof_steps,
-                "step_launches": {"kernels": "k_bulk + k_general side by side", "ms": step_launch_ms,
+                "step_launches": {"kernels": "k_bulk + k_general_walls + k_general side by side", "ms": step_launch_ms,
                                   "achieved": bytes_per_site * n_sites / (step_launch_ms * 1e-3) / 1e9},
                 "whole_step_frac": (bytes_per_site * n_sites / (ms / args.steps * 1e-3) / 1e9) / peak}
 

@@ -41,6 +41,11 @@ struct WK3Dev {           // InOutLetWK3 / InOutLetWK2 state
   int pad[2];
 };
 
+// What a step launcher launches (`which`): the plain bulk sites, all boundary
+// records, or (FP64 only) the boundary records without iolet links or those
+// with them, for launching the two on separate streams.
+constexpr int kLaunchBulk = 1, kLaunchBoundary = 2, kLaunchWallRecords = 4, kLaunchIoletRecords = 8;
+
 struct GeneralDev {
   int G;
   int G_noiolet;          // records [0, G_noiolet) have no iolet links (the first two collision-type bins)

@@ -280,11 +280,11 @@ __global__ void k_aos_to_soa(const double* aos, const int* st2ref, int n, double
 template <int K, int WALL, bool GATHER, bool MACRO>
 void launch4(const StepArgs& a, int which, int bb, int gb, cudaStream_t st) {
   if ((which & 1) && a.n > 0) k_bulk<K, GATHER, MACRO><<<(a.n + bb - 1) / bb, bb, 0, st>>>(a);
-  if ((which & 2) && a.gen.G > 0) {
-    const int g0 = a.gen.G_noiolet;
-    if (g0 > 0) k_general_walls<K, WALL, GATHER, MACRO><<<(g0 + gb - 1) / gb, gb, 0, st>>>(a);
-    if (a.gen.G > g0) k_general<K, WALL, GATHER, MACRO><<<(a.gen.G - g0 + gb - 1) / gb, gb, 0, st>>>(a, g0);
-  }
+  const int g0 = a.gen.G_noiolet;
+  if ((which & (kLaunchBoundary | kLaunchWallRecords)) && g0 > 0)
+    k_general_walls<K, WALL, GATHER, MACRO><<<(g0 + gb - 1) / gb, gb, 0, st>>>(a);
+  if ((which & (kLaunchBoundary | kLaunchIoletRecords)) && a.gen.G > g0)
+    k_general<K, WALL, GATHER, MACRO><<<(a.gen.G - g0 + gb - 1) / gb, gb, 0, st>>>(a, g0);
 }
 
 template <int K, int WALL>

@@ -117,10 +117,12 @@ Solver::Solver(LatticeTables tables, const hb_params& params, const hb_options& 
   int prio_lo = 0, prio_hi = 0;
   check(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi), "cudaDeviceGetStreamPriorityRange");
   check(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, prio_hi), "cudaStreamCreate");
+  check(cudaStreamCreateWithPriority(&side2_, cudaStreamNonBlocking, prio_hi), "cudaStreamCreate");
   check(cudaEventCreate(&ev0_), "cudaEventCreate");
   check(cudaEventCreate(&ev1_), "cudaEventCreate");
   check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "cudaEventCreate");
+  check(cudaEventCreateWithFlags(&join2_, cudaEventDisableTiming), "cudaEventCreate");
   upload();
 }
 
@@ -128,11 +130,14 @@ Solver::~Solver() {
   if (stream_) cudaStreamSynchronize(stream_);
   if (xev_) cudaEventDestroy(xev_);
   if (side_) cudaStreamSynchronize(side_);
+  if (side2_) cudaStreamSynchronize(side2_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   if (fork_) cudaEventDestroy(fork_);
   if (join_) cudaEventDestroy(join_);
+  if (join2_) cudaEventDestroy(join2_);
   if (side_) cudaStreamDestroy(side_);
+  if (side2_) cudaStreamDestroy(side2_);
   if (stream_) cudaStreamDestroy(stream_);
   if (status_host_) cudaFreeHost(status_host_);
 }
@@ -456,15 +461,24 @@ void Solver::pre_receive(bool macro, int which, bool stress) {
   }
   StepArgs a = args();
   a.pi = stress ? pi_.as<double>() : nullptr;
-  if (which == 3 && L_.G > 0) {
-    // The boundary kernel (general sites) is latency-bound and the bulk kernel
-    // bandwidth-bound: run them side by side, both after the Windkessel update.
+  // FP64 boundary records with iolet links run in their own kernel on a second
+  // side stream, beside those without (independent records, disjoint slots).
+  const bool split = !mixed() && L_.kind_start[2] > 0 && L_.kind_start[2] < L_.G;
+  if ((which & kLaunchBoundary) && L_.G > 0) {
+    // The boundary kernels are latency-bound and the bulk kernel bandwidth-bound:
+    // run them side by side, all after the Windkessel update.
     check(cudaEventRecord(fork_, stream_), "fork");
     check(cudaStreamWaitEvent(side_, fork_, 0), "fork");
-    launch(a, macro, 2, side_);
+    launch(a, macro, split ? kLaunchWallRecords : kLaunchBoundary, side_);
     check(cudaEventRecord(join_, side_), "join");
-    launch(a, macro, 1, stream_);
+    if (split) {
+      check(cudaStreamWaitEvent(side2_, fork_, 0), "fork");
+      launch(a, macro, kLaunchIoletRecords, side2_);
+      check(cudaEventRecord(join2_, side2_), "join");
+    }
+    if (which & kLaunchBulk) launch(a, macro, kLaunchBulk, stream_);
     check(cudaStreamWaitEvent(stream_, join_, 0), "join");
+    if (split) check(cudaStreamWaitEvent(stream_, join2_, 0), "join");
   } else {
     launch(a, macro, which, stream_);
   }
@@ -522,7 +536,10 @@ int Solver::step(int64_t nsteps, uint32_t flags) {
   if (shard_ && nsteps > 1)
     throw Error{HB_ERR_ARG, "a shard advances one step per call: its halo is exchanged between steps"};
   int64_t launches = 0;
-  const int per_step = (nwk3_ ? 1 : 0) + (L_.n > 0 ? 1 : 0) + (L_.G > 0 ? 1 : 0);
+  // FP64 runs the boundary records without and with iolet links as two kernels.
+  const int boundary_launches =
+      L_.G == 0 ? 0 : (mixed() ? 1 : (L_.kind_start[2] > 0 ? 1 : 0) + (L_.G > L_.kind_start[2] ? 1 : 0));
+  const int per_step = (nwk3_ ? 1 : 0) + (L_.n > 0 ? 1 : 0) + boundary_launches;
   check(cudaEventRecord(ev0_, stream_), "event");
   for (int64_t j = 0; j < nsteps; j++) {
     row_ = density_row(t_step_, nsteps - j);

@@ -134,7 +134,8 @@ class Solver {
   cudaStream_t stream_ = nullptr;
   cudaStream_t side_ = nullptr;   // boundary kernel, concurrent with the bulk kernel
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
-  cudaEvent_t fork_ = nullptr, join_ = nullptr;
+  cudaStream_t side2_ = nullptr;  // FP64: the boundary records with iolet links, beside the others
+  cudaEvent_t fork_ = nullptr, join_ = nullptr, join2_ = nullptr;
 
   DeviceBuffer f_[2];
   DeviceBuffer ghost_[2];         // iolet ghost values, paired with f_
