@@ -40,13 +40,14 @@ __device__ __forceinline__ void relax_inplace(float* g, int* status, bool trt, f
                                               float& mx, float& my, float& mz) {
   flag_unstable_status(g, status);
   moments_g(g, drho, mx, my, mz);
-  const GeqF geq(drho, mx, my, mz);
+  float eq[Q];
+  GeqF(drho, mx, my, mz).all(eq);  // the same values as GeqF::operator(), by pairs
   if (trt) {
-    g[0] = g[0] + om * (g[0] - geq(0));
+    g[0] = g[0] + om * (g[0] - eq[0]);
 #pragma unroll
     for (int i = 1; i < Q; i += 2) {
       const int j = i + 1;  // inv(i) for odd i
-      const float fi = g[i] - geq(i), fj = g[j] - geq(j);
+      const float fi = g[i] - eq[i], fj = g[j] - eq[j];
       const float gi = g[i] + 0.5f * om * (fi + fj) + 0.5f * omm * (fi - fj);
       const float gj = g[j] + 0.5f * om * (fj + fi) + 0.5f * omm * (fj - fi);
       g[i] = gi;
@@ -54,7 +55,7 @@ __device__ __forceinline__ void relax_inplace(float* g, int* status, bool trt, f
     }
   } else {
 #pragma unroll
-    for (int i = 0; i < Q; i++) g[i] = g[i] + (g[i] - geq(i)) * om;
+    for (int i = 0; i < Q; i++) g[i] = g[i] + (g[i] - eq[i]) * om;
   }
 }
 
