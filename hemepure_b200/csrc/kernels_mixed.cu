@@ -41,7 +41,8 @@ __global__ void __launch_bounds__(256) k_bulk_m2(const StepArgs a, const MixArgs
 }
 
 // Steady-state plain bulk sites of the FP16 shifted form (LBGK, TRT; no outputs),
-// SPT sites per thread (s, s + 256, ...), all gathered before any collides.
+// SPT sites per thread (s, s + 256, ...), all gathered before any collides (run
+// with one).
 // Each load is one address add: the run table row holds the plane offsets
 // i * np + run_off[i] (Solver::upload).  The collision runs on the stored
 // scale, G = kScale * g (kScale = kHalfScale for FP16, 1 for FP32), so a value
@@ -55,8 +56,10 @@ __global__ void __launch_bounds__(256) k_bulk_m2(const StepArgs a, const MixArgs
 // as before) and the stores walk one pointer by the plane stride.  4M-site
 // pipe, FP16 bulk kernel 0.0963 -> 0.0850 ms with the plane offsets, 0.0817 ms
 // with the trimmed check and stores (0.45 -> 0.52 of the measured copy
-// bandwidth), the whole FP16 step 33.1k -> 37.6k MLUPS.  Three sites per thread
-// measured slower (0.0903 ms).
+// bandwidth), the whole FP16 step 33.1k -> 37.6k MLUPS.  With the instructions
+// trimmed, one site per thread (40 registers, six blocks of 256 per SM) beats
+// two (64 registers, four blocks): 0.0826 -> 0.0779 ms, step 39.3k MLUPS; three
+// sites per thread measured 0.0903 ms, two held to 48 registers 0.0861 ms.
 template <class S>
 struct Lp;
 template <>
@@ -156,9 +159,11 @@ __global__ void __launch_bounds__(256) k_bulk_lp(const StepArgs a, const MixArgs
 // holds the gather and the BFL loads in flight together (mixed_site.cuh).
 // FP32 on the 4M pipe, time alone / whole step: eight blocks 0.0355 / 0.1231
 // ms, six 0.0326 / 0.1211 ms, five 0.0336 / 0.1227 ms; with the BFL loads
-// issued link by link and eight blocks, 0.0428 / 0.1252 ms.
+// issued link by link and eight blocks, 0.0428 / 0.1252 ms.  FP16 storage (its
+// loads half the width) runs eight: 0.0505 / 0.1021 ms at six, 0.0413 / 0.0963
+// ms at eight.
 template <class S, int K, int WALL, bool GATHER, bool MACRO>
-__global__ void __launch_bounds__(128, (K != kLES && WALL != kGZS && !MACRO) ? 6 : 1)
+__global__ void __launch_bounds__(128, (K != kLES && WALL != kGZS && !MACRO) ? (sizeof(S) == 2 ? 8 : 6) : 1)
     k_general_m(const StepArgs a, const MixArgs m) {
   const int gi = blockIdx.x * blockDim.x + threadIdx.x;
   if (gi >= a.gen.G) return;
@@ -191,7 +196,7 @@ void launch_m4(const StepArgs& a, const MixArgs& m, int which, cudaStream_t st) 
     // 4M pipe), and keeping FP32 on the general kernel's arithmetic keeps a sharded
     // FP32 lattice bit-identical to the single lattice.
     if (GATHER && !MACRO && (K == kLBGK || K == kTRT) && a.run_po && sizeof(S) == 2)
-      k_bulk_lp<S, (K == kTRT ? kTRT : kLBGK), 2><<<(a.n + 256 * 2 - 1) / (256 * 2), 256, 0, st>>>(a, m);
+      k_bulk_lp<S, (K == kTRT ? kTRT : kLBGK), 1><<<(a.n + 255) / 256, 256, 0, st>>>(a, m);
     else if (GATHER && sizeof(S) == 2) k_bulk_m2<S, K, MACRO><<<(a.n + 511) / 512, 256, 0, st>>>(a, m);
     else k_bulk_m<S, K, GATHER, MACRO><<<(a.n + 255) / 256, 256, 0, st>>>(a, m);
   }
