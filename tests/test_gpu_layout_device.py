@@ -82,3 +82,15 @@ def test_created_with_device_layout_steps_alike(case_dir, key):
     assert np.array_equal(a.GetFOld(), b.GetFOld())
     for x, y in zip(a.GetPropertyCache(), b.GetPropertyCache()):
         assert np.array_equal(x, y, equal_nan=True)
+
+
+def test_setup_timing_phases(case_dir):
+    """hb_setup_timing reports the case, geometry and solver phases of a creation
+    from a case file, and they add up to its total."""
+    xml, gmy, info, kernel, wall, steps = make_small_case(case_dir, "pipe_bfl")
+    for reader in ("device", "host"):
+        sim = lbm.LBM(xml, kernel=kernel, wall=wall, geometry_reader=reader)
+        t = sim.setup_timing()
+        assert t["geometry"] > 0.0 and t["solver"] > 0.0 and t["case"] >= 0.0
+        assert abs(t["case"] + t["geometry"] + t["solver"] - t["total"]) < 1e-6 * max(1.0, t["total"]) + 1e-9
+        sim.close()
