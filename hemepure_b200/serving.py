@@ -354,6 +354,17 @@ class Server:
                                     for r in failed]}
 
 
+def saturated_window(block_log: Sequence[Tuple[float, float, int]]) -> Dict[str, float]:
+    """Rate over the blocks run while at least half of the most members ever
+    resident were resident: block_log holds (wall seconds since the previous
+    block ended, site updates, members resident) per block."""
+    peak = max((b[2] for b in block_log), default=0)
+    sat = [b for b in block_log if peak > 0 and b[2] * 2 >= peak]
+    wall = sum(b[0] for b in sat)
+    return {"MLUPS": sum(b[1] for b in sat) / wall / 1e6 if wall > 0 else 0.0, "blocks": len(sat),
+            "wall_s": wall, "peak_resident": peak}
+
+
 def sustained_rate(requests: Sequence[Request], budget_bytes: int, tuning: Optional[Tuning] = None, device: int = 0,
                    block_steps: int = 200) -> Dict[str, float]:
     """Closed-loop saturation pass: the given requests (the head of the stream)
@@ -376,11 +387,9 @@ def sustained_rate(requests: Sequence[Request], budget_bytes: int, tuning: Optio
     srv.run(reqs)
     rep = srv.report()
     srv.close()
-    peak = max((b[2] for b in srv.block_log), default=0)
-    sat = [b for b in srv.block_log if b[2] * 2 >= peak]
-    wall = sum(b[0] for b in sat)
-    return {"MLUPS": sum(b[1] for b in sat) / wall / 1e6 if wall > 0 else rep["aggregate_MLUPS"],
-            "saturated_blocks": len(sat), "saturated_wall_s": wall, "peak_resident": peak,
+    sat = saturated_window(srv.block_log)
+    return {"MLUPS": sat["MLUPS"] if sat["wall_s"] > 0 else rep["aggregate_MLUPS"],
+            "saturated_blocks": sat["blocks"], "saturated_wall_s": sat["wall_s"], "peak_resident": sat["peak_resident"],
             "whole_pass_MLUPS": rep["aggregate_MLUPS"], "requests": len(reqs), "wall_s": rep["wall_s"],
             "device_busy_MLUPS": rep["device_busy_MLUPS"], "host_s": rep["host_s"], "device_s": rep["device_s"],
             "blocks": rep["blocks"]}

@@ -71,3 +71,15 @@ def test_dispatcher_two_worker_processes():
     assert sum(p["requests"] for p in rep["per_device"].values()) == 24
     work = sum(r.sites * r.steps for r in reqs)
     assert rep["aggregate_MLUPS"] > 0 and abs(sum(rep["assigned_work"]) - work) == 0
+
+
+def test_saturated_window_excludes_the_drain():
+    """The sustained rate counts the blocks run while at least half of the peak
+    resident set was resident: the drain at the end (one long request alone)
+    is left out, the blocks of the loaded server are in."""
+    log = [(0.5, 5e6, 8), (0.5, 5e6, 8), (0.5, 4e6, 6), (0.5, 2e6, 4), (1.0, 1e6, 1), (1.0, 1e6, 1)]
+    w = serving.saturated_window(log)
+    assert w["peak_resident"] == 8 and w["blocks"] == 4
+    assert w["wall_s"] == 2.0
+    assert abs(w["MLUPS"] - 16e6 / 2.0 / 1e6) < 1e-12
+    assert serving.saturated_window([])["blocks"] == 0
