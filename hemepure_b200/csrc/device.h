@@ -42,8 +42,8 @@ struct WK3Dev {           // InOutLetWK3 / InOutLetWK2 state
 };
 
 // What a step launcher launches (`which`): the plain bulk sites, all boundary
-// records, or (FP64 only) the boundary records without iolet links or those
-// with them, for launching the two on separate streams.
+// records, or the boundary records without iolet links or those with them, for
+// launching the two on separate streams.
 constexpr int kLaunchBulk = 1, kLaunchBoundary = 2, kLaunchWallRecords = 4, kLaunchIoletRecords = 8;
 
 struct GeneralDev {

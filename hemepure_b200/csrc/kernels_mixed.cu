@@ -164,10 +164,20 @@ __global__ void __launch_bounds__(256) k_bulk_lp(const StepArgs a, const MixArgs
 // ms at eight.
 template <class S, int K, int WALL, bool GATHER, bool MACRO>
 __global__ void __launch_bounds__(128, (K != kLES && WALL != kGZS && !MACRO) ? (sizeof(S) == 2 ? 8 : 6) : 1)
-    k_general_m(const StepArgs a, const MixArgs m) {
-  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    k_general_m(const StepArgs a, const MixArgs m, int g0) {
+  const int gi = g0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (gi >= a.gen.G) return;
   general_site_m<S, K, WALL, GATHER, MACRO>(a, m, gi);
+}
+
+// The records without iolet links, compiled without the iolet rules (as the
+// FP64 k_general_walls); k_general_m takes the rest beside it.
+template <class S, int K, int WALL, bool GATHER, bool MACRO>
+__global__ void __launch_bounds__(128, (K != kLES && WALL != kGZS && !MACRO) ? (sizeof(S) == 2 ? 8 : 6) : 1)
+    k_general_m_walls(const StepArgs a, const MixArgs m) {
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi >= a.gen.G_noiolet) return;
+  general_site_m<S, K, WALL, GATHER, MACRO, false>(a, m, gi);
 }
 
 template <class S, int WALL, bool GATHER>
@@ -200,7 +210,11 @@ void launch_m4(const StepArgs& a, const MixArgs& m, int which, cudaStream_t st) 
     else if (GATHER && sizeof(S) == 2) k_bulk_m2<S, K, MACRO><<<(a.n + 511) / 512, 256, 0, st>>>(a, m);
     else k_bulk_m<S, K, GATHER, MACRO><<<(a.n + 255) / 256, 256, 0, st>>>(a, m);
   }
-  if ((which & 2) && a.gen.G > 0) k_general_m<S, K, WALL, GATHER, MACRO><<<(a.gen.G + 127) / 128, 128, 0, st>>>(a, m);
+  const int g0 = a.gen.G_noiolet;
+  if ((which & (kLaunchBoundary | kLaunchWallRecords)) && g0 > 0)
+    k_general_m_walls<S, K, WALL, GATHER, MACRO><<<(g0 + 127) / 128, 128, 0, st>>>(a, m);
+  if ((which & (kLaunchBoundary | kLaunchIoletRecords)) && a.gen.G > g0)
+    k_general_m<S, K, WALL, GATHER, MACRO><<<(a.gen.G - g0 + 127) / 128, 128, 0, st>>>(a, m, g0);
 }
 
 template <class S, int K, int WALL>

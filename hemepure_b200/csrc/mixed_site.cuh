@@ -253,10 +253,10 @@ __device__ __forceinline__ void gather_bulk_m(const StepArgs& a, const MixArgs& 
 // link, g*_d of the own site for a wall link, g*_i of the source site otherwise
 // (s + run offset for a record that follows its run, else its pull table).  The
 // BFL correction of wall links follows as a predicated step (as the FP64 kernel).
-template <class S, int WALL>
+template <class S, int WALL, bool IO = true>
 __device__ __forceinline__ void gather_general_m(const StepArgs& a, const MixArgs& m, int gi, int s, float* g) {
   const GeneralDev& G = a.gen;
-  const uint32_t wm = __ldg(G.wall + gi), im = __ldg(G.iolet + gi);
+  const uint32_t wm = __ldg(G.wall + gi), im = IO ? __ldg(G.iolet + gi) : 0u;
   const int run = __ldg(G.run + gi);
   int src[18];
   if (run >= 0) {
@@ -381,13 +381,13 @@ __device__ __forceinline__ void bulk_site_m(const StepArgs& a, const MixArgs& m,
 }
 
 // One general site gi (k_general_m, and the batched kernel).
-template <class S, int K, int WALL, bool GATHER, bool MACRO>
+template <class S, int K, int WALL, bool GATHER, bool MACRO, bool IO = true>
 __device__ __forceinline__ void general_site_m(const StepArgs& a, const MixArgs& m, int gi) {
   const GeneralDev& G = a.gen;
   const int s = __ldg(G.site + gi);
-  const uint32_t wm = __ldg(G.wall + gi), im = __ldg(G.iolet + gi);
+  const uint32_t wm = __ldg(G.wall + gi), im = IO ? __ldg(G.iolet + gi) : 0u;
   float g[Q];
-  if (GATHER) gather_general_m<S, WALL>(a, m, gi, s, g);
+  if (GATHER) gather_general_m<S, WALL, IO>(a, m, gi, s, g);
   else {
 #pragma unroll
     for (int i = 0; i < Q; i++) g[i] = ldg_s<S>(m, (int64_t)i * a.np + s);

@@ -134,7 +134,7 @@ class Solver {
   cudaStream_t stream_ = nullptr;
   cudaStream_t side_ = nullptr;   // boundary kernel, concurrent with the bulk kernel
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
-  cudaStream_t side2_ = nullptr;  // FP64: the boundary records with iolet links, beside the others
+  cudaStream_t side2_ = nullptr;  // the boundary records with iolet links, beside the others
   cudaEvent_t fork_ = nullptr, join_ = nullptr, join2_ = nullptr;
 
   DeviceBuffer f_[2];
@@ -151,7 +151,11 @@ class Solver {
   DeviceBuffer sum_scratch_, sum_out_;
   int dens_rows_ = 0;
   int row_ = 0;                   // row of the density table used by the current step
-  std::vector<double> host_rows_;
+  // Pinned, so a step's row upload is a direct asynchronous copy; rows_ev_ marks
+  // when the last upload has read it, before the next fill rewrites it.
+  double* host_rows_ = nullptr;
+  cudaEvent_t rows_ev_ = nullptr;
+  bool rows_pending_ = false;
   bool rows_valid_ = false;         // the device table holds the rows of steps rows_first_ ...
   uint64_t rows_first_ = 0;
   int rows_count_ = 0;              // rows uploaded at rows_first_
